@@ -1,0 +1,306 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 Lucas-Lehmer engine; prints ONE JSON line (rank 0).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload range|...] [--impl b200|reference]
+
+Workloads (synthetic inputs are the exponents themselves, from the sieve; s_0 = 4):
+  range   every prime p <= 100,001 (9,592 Lucas-Lehmer tests, 28 Mersenne hits), batched whole-test
+          kernels bucketed by transform length. One step = every test run to completion.
+          metric: tests/s (higher is better).
+
+value: tests/s with the job lists already resident on the device (CUDA events recorded on the
+launch stream around each step; the L2 is flushed with a 512 MiB write between steps).
+e2e:   the same metric through the reference-facing call lucaslehmer_cuda.lucas_lehmer_batch(),
+       host lists in, (p, is_prime, seconds, res64) out, every host<->device copy and the exact
+       residue rebuild inside the timed region.
+--impl reference: the reference's own CPU engine (its lucaslehmer.cpp compiled unchanged into
+oracle/_ref/, GMP engine) on the host cores, on a bounded stratified sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "mersenneprime_python_cpp_gmp_benchmark_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+RANGE_HI = 100001
+METRIC_RANGE = "tests/s for all p<=100001 (residues exact)"
+
+
+def sieve(lo, hi):
+    comp = bytearray(hi + 1)
+    i = 2
+    while i * i <= hi:
+        if not comp[i]:
+            comp[i * i::i] = b"\x01" * len(range(i * i, hi + 1, i))
+        i += 1
+    return [i for i in range(max(lo, 2), hi + 1) if not comp[i]]
+
+
+# ---- clocks sampled during the timed region ------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = max(smax, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---- distributed plumbing ------------------------------------------------------------------
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    if torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=datetime.timedelta(seconds=600))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+class L2Flush:
+    """Writes a buffer larger than the 126 MB L2 between timed steps."""
+
+    def __init__(self):
+        import torch
+        self.buf = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def __call__(self):
+        import torch
+        self.buf.fill_(1.0)
+        torch.cuda.synchronize()
+
+
+# ---- the range workload ------------------------------------------------------------------
+
+def range_flops(results):
+    """Algorithmic FP64 flops of the tests: 5 N log2 N per squaring (forward + inverse real FFT)."""
+    tot = 0.0
+    for r in results:
+        n = r["n"]
+        if n >= 32:
+            tot += r["iters"] * 5.0 * n * (n.bit_length() - 1)
+    return tot
+
+
+def bench_range(args, rank, world):
+    import torch
+    from mersenneprime_python_cpp_gmp_benchmark_b200 import llgpu
+    ps_all = sieve(2, RANGE_HI)
+    mine = sorted(ps_all, reverse=True)[rank::world]  # round-robin over descending p: balanced shards
+    batch = llgpu.Batch(mine)
+    flush = L2Flush()
+    for _ in range(args.warmup):
+        batch.launch()
+        batch.device_ms()
+    res = batch.results()
+    known = {int(x) for x in open(os.path.join(ROOT, "tests", "golden", "known_mp_list.txt")).read().split()}
+    hits = sorted(r["p"] for r in res if r["is_zero"])
+    assert all(r["status"] == 0 for r in res), "a test failed"
+    assert set(hits) == {p for p in known if p in set(mine)}, "hit set differs from known_mp_list.txt"
+    barrier(world)
+    torch.cuda.synchronize()
+    times = []
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        for _ in range(args.steps):
+            flush()
+            batch.launch()
+            times.append(batch.device_ms() * 1e-3)
+    torch.cuda.synchronize()
+    barrier(world)
+    t_rank = sum(times)
+    t_max = max_over_ranks(t_rank, world)
+    tests = sum_over_ranks(len(mine) * args.steps, world)
+    value = tests / t_max
+    # e2e through the reference-facing call (host lists in, results out)
+    import lucaslehmer_cuda as lc
+    lc.lucas_lehmer_batch(mine[:64])
+    t0 = time.perf_counter()
+    out = lc.lucas_lehmer_batch(mine)
+    t_e2e = time.perf_counter() - t0
+    assert sorted(p for p, r, s, res64 in out if r) == hits
+    t_e2e = max_over_ranks(t_e2e, world)
+    e2e = sum_over_ranks(len(mine), world) / t_e2e
+    h2d = 16 * len(mine)
+    d2h = sum(8 * r["n"] + 32 for r in res)
+    flops = range_flops(res)
+    achieved = flops / (t_rank / args.steps) / 1e12
+    peak = llgpu.measure_peak("fp64") / 1e12
+    line = {
+        "metric": METRIC_RANGE, "value": round(value, 2), "unit": "tests/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * t_max / args.steps, 3),
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: every prime exponent p <= 100001 from the sieve, s_0 = 4",
+        "config": {"workload": "range p<=100001 (9592 LL tests, batched whole-test kernels, FP64 IBDWT, "
+                               "pow2 N 32..8192 at <=18 bits/digit)",
+                   "tests": len(ps_all), "l2": "flushed (512 MiB write) between steps",
+                   "parallelism": f"exponents sharded round-robin over {world} GPU(s)"},
+        "e2e": {"value": round(e2e, 2), "unit": "tests/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "fp64", "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "TFLOP/s",
+                     "frac": round(achieved / peak, 4),
+                     "peak_source": "measured FP64 FMA probe (llg_measure_peak)", "traffic": None,
+                     "work": "5 N log2 N flops per squaring x (p-2) squarings, summed over the range"},
+        "clocks": clk.summary(),
+        "hits": len(hits),
+    }
+    return line
+
+
+def cpu_baseline_range(threads, budget_s=20.0):
+    """Reference GMP engine (oracle/_ref, compiled unchanged) on a stratified sample of the range."""
+    from oracle import oracle
+    ref = oracle.reference_module()
+    kind = "reference"
+    if ref is None:
+        kind = "port"
+    ps = sieve(2, RANGE_HI)
+    # stratified: every k-th prime; grow k until the sample fits the budget (cost ~ p^2.3)
+    k = 64
+    est = lambda kk: sum((p / 1e5) ** 2.3 * 9.0 for p in ps[::kk]) / threads  # ~9 s per p=1e5 test
+    while est(k) > budget_s and k < 4096:
+        k *= 2
+    sample = ps[k // 2::k]
+    run = (lambda p: ref.lucas_lehmer_res(p)) if ref else (lambda p: oracle.ll_gmp(p)[:2])
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(run, sorted(sample, reverse=True)))
+    wall = time.perf_counter() - t0
+    est_wall = wall * k
+    return {"value": round(len(ps) / est_wall, 4), "unit": "tests/s", "cores": threads, "kind": kind,
+            "sample": f"reference GMP engine (lucaslehmer_res) on every {k}th prime p<=100001 "
+                      f"({len(sample)} tests, {wall:.1f} s wall on {threads} threads); full-range wall "
+                      f"extrapolated as sample wall x {k}"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", choices=("range",), default="range")
+    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    threads = os.cpu_count() or 1
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        if rank != 0:
+            return 0
+        t0 = time.perf_counter()
+        vals = []
+        for _ in range(args.warmup):
+            pass  # the reference engine has no warm-up state; warm-up steps are not repeated on CPU
+        for _ in range(args.steps):
+            vals.append(cpu_baseline_range(threads, budget_s=15.0))
+        v = statistics.median(x["value"] for x in vals)
+        line = {"metric": METRIC_RANGE, "value": v, "unit": "tests/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "int64 (GMP limbs)", "data": "synthetic",
+                "config": {"workload": "range p<=100001 (9592 LL tests)"}, "impl": "reference",
+                "cpu_baseline": vals[-1], "e2e": {"value": v, "unit": "tests/s", "h2d_bytes_per_step": 0,
+                                                   "d2h_bytes_per_step": 0},
+                "ms_per_step": round(1e3 * (time.perf_counter() - t0) / max(1, args.steps), 1)}
+        print(json.dumps(line))
+        return 0
+    rank, world, local = dist_setup(args.gpus)
+    line = bench_range(args, rank, world)
+    if rank == 0:
+        if not args.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline_range(threads)
+        line["gpu_launches"] = (args.steps) * 9  # one whole-test launch per length group per step
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,126 @@
+/* llgpu: B200 (sm_100a) Lucas-Lehmer squaring engine -- the C-ABI drop-in boundary.
+ *
+ * Plain C types only (no CUDA or torch types): pointers, sizes, status codes. Every function is
+ * callable from many host threads at once; each host thread gets its own CUDA stream and device
+ * buffers. All results are exact: floating-point runs whose round-off ever exceeds the abort
+ * threshold are redone at a longer transform on the GPU (no CPU fallback).
+ *
+ * Each entry point names the reference interface it replaces (wadeghcp/MersennePrime_Python_CPP_
+ * GMP_BenchMark; file:line). The reference binds those functions to Python with pybind11
+ * (lucaslehmer.cpp:344-387, cuda/ll_ntt.cu:274-281); this library's pybind11 modules
+ * (lucaslehmer, lucaslehmer_cuda) bind these entry points the same way.
+ */
+#ifndef LLGPU_H
+#define LLGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LLG_ABI_VERSION 1
+
+/* Status codes (return values and llg_result.status). */
+enum {
+    LLG_OK = 0,
+    LLG_E_CUDA = 1,        /* a CUDA runtime call failed (message: llg_last_error()) */
+    LLG_E_NODEV = 2,       /* no CUDA device visible */
+    LLG_E_ARG = 3,         /* invalid argument (null pointer, size too small, bad engine) */
+    LLG_E_UNSUPPORTED = 4, /* exponent / length outside what the engine handles */
+    LLG_E_ROUNDOFF = 5,    /* round-off stayed above the threshold at every length tried */
+    LLG_E_TIMEOUT = 6,     /* a bounded device-side wait gave up */
+    LLG_E_NOMEM = 7        /* device allocation failed */
+};
+
+/* Engines. FP64 = Crandall-Fagin IBDWT in double precision (lucaslehmer.cpp:209-342);
+ * NTT = the same digit layout in GF(2^64 - 2^32 + 1), exact (cuda/ll_ntt.cu). */
+enum { LLG_ENGINE_FP64 = 0, LLG_ENGINE_NTT = 1 };
+
+typedef struct llg_result {
+    uint64_t p;
+    uint64_t iters;       /* squarings performed: p-2, or the requested interim count */
+    uint64_t res64;       /* low 64 bits of s_iters mod 2^p - 1, in [0, 2^p - 1) */
+    double max_err;       /* worst |x - round(x)| over the run (FP64; 0 for NTT) */
+    double seconds;       /* device time of the test */
+    uint32_t n;           /* transform length that produced the result */
+    uint32_t escalations; /* times the length was raised after a round-off abort */
+    int32_t is_zero;      /* residue == 0; for a full run: 2^p - 1 is prime */
+    int32_t status;       /* LLG_OK or an LLG_E_* code for this exponent */
+} llg_result;
+
+/* Human-readable text of a status code; llg_last_error(): detail of this thread's last failure. */
+const char* llg_status_string(int status);
+const char* llg_last_error(void);
+
+/* (name, SM count, global memory) of the current device.
+ * Replaces device_info(), cuda/ll_ntt.cu:269-272. */
+int llg_device_info(char* name, size_t name_cap, int* sms, uint64_t* total_mem);
+
+/* Transform length the FP64 engine uses for p at <= max_bpw bits per digit (<= 0: the module
+ * default, see llg_set_max_bpw); 0 = p outside the engine's range.
+ * Replaces fft_length(), lucaslehmer.cpp:244-254. */
+uint32_t llg_fft_length(uint64_t p, double max_bpw);
+/* Default bits-per-digit bound of llg_fft_length (18 unless changed).
+ * Replaces set_fft_bits_per_word(), lucaslehmer.cpp:368 (g_max_bpw, lucaslehmer.cpp:246). */
+int llg_set_max_bpw(double bpw);
+double llg_get_max_bpw(void);
+/* NTT length for p (exactness bound ceil(p/N) <= (63 - log2 N)/2); 0 = cannot take.
+ * Replaces ntt_length(), cuda/ll_ntt.cu:172-180. */
+uint32_t llg_ntt_length(uint64_t p);
+/* Largest exponent an engine handles. Replaces max_exponent(), cuda/ll_ntt.cu:279. */
+uint64_t llg_max_exponent(int engine);
+
+/* One Lucas-Lehmer test (max_iters == 0) or its first max_iters squarings, on the GPU.
+ * n == 0 picks the length (llg_fft_length / llg_ntt_length). words (optional, nwords >=
+ * ceil(p/64)): the full residue s_iters mod 2^p - 1, little-endian 64-bit limbs.
+ * Replaces lucas_lehmer_fft_raw() + the GMP rebuild, lucaslehmer.cpp:257-329, and, for the exact
+ * engine, lucas_lehmer_n(), lucaslehmer.cpp:29-58. */
+int llg_run(uint64_t p, uint64_t max_iters, int engine, uint32_t n, llg_result* out,
+            uint64_t* words, size_t nwords);
+
+/* Many exponents in one call: grouped by transform length, one batched launch per group, the
+ * groups running concurrently. out[i] corresponds to ps[i]. words_out (optional): for each i,
+ * ceil(ps[i]/64) limbs, concatenated in input order.
+ * Replaces lucas_lehmer_batch() / run_batch(), cuda/ll_ntt.cu:198-267. */
+int llg_run_batch(const uint64_t* ps, size_t count, uint64_t max_iters, int engine,
+                  llg_result* out, uint64_t* words_out, size_t words_cap);
+
+/* Device-resident batches: the same work as llg_run_batch split into create (upload the job
+ * lists, allocate), launch (enqueue every length group on its own stream, forked from and joined
+ * back into `stream`, so events recorded on `stream` bracket the whole batch; stream == NULL uses
+ * a per-thread stream) and results (wait, read back, redo round-off aborts at longer lengths,
+ * rebuild residues). A batch may be launched again after its results are read.
+ * flags: LLG_BATCH_KEEP_WORDS keeps full residues for llg_batch_results; LLG_BATCH_ERRLOG keeps
+ * the per-iteration max round-off of a single-exponent batch for llg_batch_errlog.
+ * Replaces run_batch()'s upload / launch / readback phases, cuda/ll_ntt.cu:213-235. */
+typedef struct llg_batch llg_batch;
+#define LLG_BATCH_KEEP_WORDS 1
+#define LLG_BATCH_ERRLOG 2
+int llg_batch_create(const uint64_t* ps, size_t count, uint64_t max_iters, int engine, int flags,
+                     llg_batch** out);
+int llg_batch_launch(llg_batch* b, void* stream);
+int llg_batch_results(llg_batch* b, llg_result* out, uint64_t* words, size_t words_cap);
+int llg_batch_errlog(llg_batch* b, float* log, size_t cap, size_t* len);
+/* Device time of the last launch: CUDA events recorded on the launch stream before the fork and
+ * after the join (waits for the launch to finish). */
+int llg_batch_device_ms(llg_batch* b, float* ms);
+void llg_batch_destroy(llg_batch* b);
+
+/* Exact residue of balanced (or any signed) digits: s = sum_j d_j 2^ceil(jp/n) mod 2^p - 1.
+ * Host-only; needs no GPU. Replaces the GMP rebuild, lucaslehmer.cpp:312-323 and
+ * cuda/ll_ntt.cu:238-252. Returns LLG_OK; *is_zero set when s == 0. */
+int llg_residue_from_digits(uint64_t p, uint32_t n, const int64_t* digits, uint64_t* words,
+                            size_t nwords, uint64_t* res64, int32_t* is_zero);
+
+/* Roofline denominators measured on the current device: which = 0 FP64 FMA flops/s,
+ * which = 1 INT32 multiply-adds/s (dependent chains on every SM). Diagnostic; no reference
+ * counterpart. */
+int llg_measure_peak(int which, double* ops_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,589 @@
+// The C-ABI boundary (include/llgpu.h): engine selection, transform-length choice, per-thread
+// CUDA streams and buffers, the round-off escalation loop and the exact residue rebuild.
+// Everything numerical runs on the GPU; the host only sizes, launches, and turns digits into the
+// residue (llg_residue.cpp). There is no CPU fallback: a CUDA failure is an error status.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/llgpu.h"
+#include "llg_internal.h"
+
+namespace {
+
+using namespace llg;
+
+thread_local std::string t_last_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    t_last_error = buf;
+    return code;
+}
+
+#define CK(x)                                                                                 \
+    do {                                                                                      \
+        cudaError_t e_ = (x);                                                                 \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(e_ == cudaErrorMemoryAllocation ? LLG_E_NOMEM : LLG_E_CUDA,           \
+                        "CUDA: %s at %s (%s:%d)", cudaGetErrorString(e_), #x, __FILE__, __LINE__); \
+    } while (0)
+
+double g_max_bpw = 18.0;  // lucaslehmer.cpp:246
+std::mutex g_mx;
+const double kAbortErr = 0.4;
+
+constexpr int kSmallLogMin = 5;   // N = 32
+constexpr int kSmallLogMax = 13;  // N = 8192
+
+// ---- device tables ------------------------------------------------------------------------
+
+struct DeviceTables {
+    double2* qtw[kSmallLogMax + 1] = {};  // quarter-wave twiddles of the M = N/2 point FFT
+};
+std::map<int, DeviceTables> g_tables;  // per device ordinal
+
+int device_ready(int* dev_out) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return fail(LLG_E_NODEV, "no CUDA device visible (%s)",
+                    e != cudaSuccess ? cudaGetErrorString(e) : "device count 0");
+    }
+    CK(cudaGetDevice(dev_out));
+    return LLG_OK;
+}
+
+// e^{-2 pi i r / M}, r < M/4, rounded once from long double.
+std::vector<double2> quarter_table(int log_m) {
+    const size_t M = (size_t)1 << log_m, Q = M / 4;
+    std::vector<double2> q(Q);
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    for (size_t r = 0; r < Q; ++r) {
+        long double a = two_pi * (long double)r / (long double)M;
+        q[r] = make_double2((double)cosl(a), -(double)sinl(a));
+    }
+    return q;
+}
+
+int get_qtw(int dev, int log_m, const double2** out) {
+    std::lock_guard<std::mutex> lk(g_mx);
+    DeviceTables& T = g_tables[dev];
+    if (!T.qtw[log_m]) {
+        std::vector<double2> h = quarter_table(log_m);
+        double2* d = nullptr;
+        CK(cudaMalloc(&d, h.size() * sizeof(double2)));
+        CK(cudaMemcpy(d, h.data(), h.size() * sizeof(double2), cudaMemcpyHostToDevice));
+        T.qtw[log_m] = d;
+    }
+    *out = T.qtw[log_m];
+    return LLG_OK;
+}
+
+// ---- lengths --------------------------------------------------------------------------------
+
+int ilog2_exact(uint64_t n) {
+    if (n == 0 || (n & (n - 1))) return -1;
+    int l = 0;
+    while ((1ull << l) < n) ++l;
+    return l;
+}
+
+constexpr uint64_t kMaxDigitBits = 28;  // FP64 digits are held as int32 between iterations
+constexpr uint64_t kWordMaxP = 256;     // p below this runs on the exact multi-limb word kernel
+
+// A length is usable when every digit has enough bits for the one-exchange balanced carry to stay
+// balanced (floor(p/N) >= log2(N)/2 + 2: the carry into a digit is ~sqrt(N) times smaller than its
+// base) and few enough for int32 digits and FP64 products.
+bool fp64_length_usable(uint64_t p, uint64_t n) {
+    const int l = ilog2_exact(n);
+    if (l < kSmallLogMin || l > kSmallLogMax) return false;
+    return 2 * (p / n) >= (uint64_t)l + 4 && (p + n - 1) / n <= kMaxDigitBits;
+}
+
+// smallest usable length with p / N <= bpw
+uint32_t fp64_length(uint64_t p, double bpw) {
+    for (int l = kSmallLogMin; l <= kSmallLogMax; ++l) {
+        const uint64_t N = 1ull << l;
+        if ((double)p / (double)N <= bpw && fp64_length_usable(p, N)) return (uint32_t)N;
+    }
+    return 0;
+}
+
+uint32_t next_fp64_length(uint64_t p, uint32_t n) {
+    for (int l = kSmallLogMin; l <= kSmallLogMax; ++l) {
+        const uint64_t N = 1ull << l;
+        if (N > n && fp64_length_usable(p, N)) return (uint32_t)N;
+    }
+    return 0;
+}
+
+// ---- batches: exponents grouped by length, one launch per group, groups on their own streams --
+
+struct Item {
+    size_t idx;  // position in the caller's arrays
+    uint64_t p;
+    uint64_t iters;
+    uint32_t n;  // 0: word path (p < 64)
+    uint32_t escalations;
+};
+
+struct Group {
+    uint32_t n = 0;  // 0 = word path
+    std::vector<Item> items;
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+    void* d_jobs = nullptr;
+    void* d_results = nullptr;  // SmallResult[] or uint64_t[] (word path)
+    void* d_digits = nullptr;
+};
+
+void set_trivial(llg_result* r, uint64_t p) {
+    std::memset(r, 0, sizeof *r);
+    r->p = p;
+    r->status = LLG_OK;
+    r->is_zero = (p == 2) ? 1 : 0;  // lucaslehmer.cpp:31-33: p<2 and even p composite, p=2 prime
+}
+
+}  // namespace
+
+struct llg_batch {
+    int dev = -1;
+    int engine = LLG_ENGINE_FP64;
+    size_t count = 0;
+    std::vector<uint64_t> ps;
+    std::vector<llg_result> out;
+    std::vector<Group> groups;
+    cudaEvent_t fork = nullptr;   // recorded on the caller's stream at launch (timing enabled)
+    cudaEvent_t joined = nullptr; // recorded on the caller's stream after every group joined
+    bool launched = false;
+    bool collected = false;
+    bool keep_words = false;
+    std::vector<std::vector<uint64_t>> words;  // per exponent, when keep_words
+    float* d_errlog = nullptr;  // optional per-iteration round-off log (single-exponent batches)
+    uint64_t errlog_len = 0;
+};
+
+namespace {
+
+void release_group(Group& g) {
+    if (g.st) {
+        if (g.d_jobs) cudaFreeAsync(g.d_jobs, g.st);
+        if (g.d_results) cudaFreeAsync(g.d_results, g.st);
+        if (g.d_digits) cudaFreeAsync(g.d_digits, g.st);
+        cudaStreamSynchronize(g.st);
+        cudaStreamDestroy(g.st);
+    }
+    if (g.done) cudaEventDestroy(g.done);
+    g = Group();
+}
+
+void destroy_batch(llg_batch* b) {
+    if (!b) return;
+    for (Group& g : b->groups) release_group(g);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->joined) cudaEventDestroy(b->joined);
+    if (b->d_errlog) cudaFree(b->d_errlog);
+    delete b;
+}
+
+// Allocates and uploads one group's job list (synchronously on the group's stream).
+int setup_group(Group& g) {
+    CK(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
+    const size_t cnt = g.items.size();
+    // longest first: the block scheduler then hands out the tests in LPT order
+    std::sort(g.items.begin(), g.items.end(), [](const Item& a, const Item& b) { return a.iters > b.iters; });
+    std::vector<SmallJob> jobs(cnt);
+    for (size_t i = 0; i < cnt; ++i) jobs[i] = SmallJob{g.items[i].p, g.items[i].iters};
+    CK(cudaMallocAsync(&g.d_jobs, cnt * sizeof(SmallJob), g.st));
+    if (g.n == 0) {
+        CK(cudaMallocAsync(&g.d_results, cnt * 4 * sizeof(uint64_t), g.st));
+    } else {
+        CK(cudaMallocAsync(&g.d_results, cnt * sizeof(SmallResult), g.st));
+        CK(cudaMallocAsync(&g.d_digits, cnt * (size_t)g.n * sizeof(int64_t), g.st));
+    }
+    CK(cudaMemcpyAsync(g.d_jobs, jobs.data(), cnt * sizeof(SmallJob), cudaMemcpyHostToDevice, g.st));
+    CK(cudaStreamSynchronize(g.st));
+    return LLG_OK;
+}
+
+int launch_group(llg_batch* b, Group& g, cudaStream_t caller) {
+    CK(cudaStreamWaitEvent(g.st, b->fork, 0));
+    const int cnt = (int)g.items.size();
+    if (g.n == 0) {
+        CK(launch_word((const SmallJob*)g.d_jobs, cnt, (uint64_t*)g.d_results, g.st));
+    } else {
+        const double2* qtw = nullptr;
+        int rc = get_qtw(b->dev, ilog2_exact(g.n) - 1, &qtw);
+        if (rc) return rc;
+        float* elog = (cnt == 1) ? b->d_errlog : nullptr;
+        CK(launch_small_fp64(ilog2_exact(g.n), (const SmallJob*)g.d_jobs, cnt, qtw, (int64_t*)g.d_digits,
+                             (SmallResult*)g.d_results, elog, kAbortErr, g.st));
+    }
+    CK(cudaEventRecord(g.done, g.st));
+    CK(cudaStreamWaitEvent(caller, g.done, 0));
+    return LLG_OK;
+}
+
+// Reads one finished group back; items that aborted on round-off go to `retry` at a longer length.
+int collect_group(llg_batch* b, Group& g, std::vector<Item>& retry) {
+    const size_t cnt = g.items.size();
+    CK(cudaEventSynchronize(g.done));
+    if (g.n == 0) {
+        std::vector<uint64_t> res(cnt * 4);
+        CK(cudaMemcpyAsync(res.data(), g.d_results, cnt * 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost, g.st));
+        CK(cudaStreamSynchronize(g.st));
+        for (size_t i = 0; i < cnt; ++i) {
+            llg_result& r = b->out[g.items[i].idx];
+            const uint64_t* w = res.data() + 4 * i;
+            const size_t nw = (size_t)((g.items[i].p + 63) / 64);
+            if (b->keep_words) b->words[g.items[i].idx].assign(w, w + nw);
+            r.iters = g.items[i].iters;
+            r.res64 = w[0];
+            r.is_zero = (w[0] | w[1] | w[2] | w[3]) == 0;
+            r.n = 1;
+            r.status = LLG_OK;
+        }
+        return LLG_OK;
+    }
+    const uint32_t n = g.n;
+    std::vector<SmallResult> res(cnt);
+    std::vector<int64_t> digits(cnt * (size_t)n);
+    CK(cudaMemcpyAsync(res.data(), g.d_results, cnt * sizeof(SmallResult), cudaMemcpyDeviceToHost, g.st));
+    CK(cudaMemcpyAsync(digits.data(), g.d_digits, digits.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, g.st));
+    CK(cudaStreamSynchronize(g.st));
+    for (size_t i = 0; i < cnt; ++i) {
+        const Item& it = g.items[i];
+        llg_result& r = b->out[it.idx];
+        r.max_err = std::max(r.max_err, res[i].max_err);
+        r.seconds += (double)res[i].ns * 1e-9;
+        if (res[i].status == LLG_ST_ROUNDOFF) {
+            const uint32_t nn = next_fp64_length(it.p, n);
+            r.n = n;
+            r.escalations = it.escalations;
+            if (!nn) {
+                r.status = LLG_E_ROUNDOFF;
+                continue;
+            }
+            Item again = it;
+            again.n = nn;
+            again.escalations++;
+            retry.push_back(again);
+            continue;
+        }
+        r.iters = res[i].iters_done;
+        r.n = n;
+        r.escalations = it.escalations;
+        int32_t z = 0;
+        uint64_t* w = nullptr;
+        const size_t nw = (size_t)((it.p + 63) / 64);
+        if (b->keep_words) {
+            b->words[it.idx].assign(nw, 0);
+            w = b->words[it.idx].data();
+        }
+        const int rc = llg_residue_from_digits(it.p, n, digits.data() + i * (size_t)n, w, nw, &r.res64, &z);
+        if (rc) return rc;
+        r.is_zero = z;
+        r.status = LLG_OK;
+    }
+    return LLG_OK;
+}
+
+// Creates a batch: trivial exponents resolved on the host, the rest grouped by length.
+// strict: a single-exponent call fails on an unsupported exponent; a batch marks it and goes on
+// (the reference's batch returns such exponents with seconds < 0, cuda/ll_ntt.cu:259-267).
+int make_batch(const uint64_t* ps, size_t count, uint64_t max_iters, int engine, uint32_t n_force,
+               bool strict, int flags, llg_batch** outb) {
+    if (engine != LLG_ENGINE_FP64) return fail(LLG_E_UNSUPPORTED, "engine %d not available", engine);
+    int dev;
+    int rc = device_ready(&dev);
+    if (rc) return rc;
+    llg_batch* b = new llg_batch();
+    b->dev = dev;
+    b->engine = engine;
+    b->count = count;
+    b->ps.assign(ps, ps + count);
+    b->out.resize(count);
+    b->keep_words = (flags & LLG_BATCH_KEEP_WORDS) != 0;
+    if (b->keep_words) b->words.resize(count);
+    std::map<uint32_t, std::vector<Item>> groups;
+    for (size_t i = 0; i < count; ++i) {
+        const uint64_t p = ps[i];
+        set_trivial(&b->out[i], p);
+        if (p < 3 || p % 2 == 0) continue;  // decided without iterating (lucaslehmer.cpp:31-33)
+        const uint64_t full = p - 2;
+        const uint64_t iters = (max_iters && max_iters < full) ? max_iters : full;
+        b->out[i].iters = iters;
+        Item it{i, p, iters, 0, 0};
+        if (p >= kWordMaxP) {
+            uint32_t n = n_force;
+            if (n_force && !fp64_length_usable(p, n_force)) {
+                destroy_batch(b);
+                return fail(LLG_E_UNSUPPORTED, "length %u not usable for p=%llu", n_force, (unsigned long long)p);
+            }
+            if (!n) n = fp64_length(p, g_max_bpw);
+            if (!n) {
+                b->out[i].status = LLG_E_UNSUPPORTED;
+                if (strict) {
+                    destroy_batch(b);
+                    return fail(LLG_E_UNSUPPORTED, "p=%llu above the engine's range", (unsigned long long)p);
+                }
+                continue;
+            }
+            it.n = n;
+        }
+        groups[it.n].push_back(it);
+    }
+    for (auto& kv : groups) {
+        Group g;
+        g.n = kv.first;
+        g.items = std::move(kv.second);
+        b->groups.push_back(std::move(g));
+    }
+    // largest lengths first (they run longest)
+    std::sort(b->groups.begin(), b->groups.end(), [](const Group& x, const Group& y) { return x.n > y.n; });
+    for (Group& g : b->groups) {
+        if ((rc = setup_group(g))) {
+            destroy_batch(b);
+            return rc;
+        }
+    }
+    cudaError_t e = cudaEventCreate(&b->fork);
+    if (e == cudaSuccess) e = cudaEventCreate(&b->joined);
+    if (e == cudaSuccess && (flags & LLG_BATCH_ERRLOG) && b->groups.size() == 1 &&
+        b->groups[0].items.size() == 1 && b->groups[0].n) {
+        b->errlog_len = b->groups[0].items[0].iters;
+        e = cudaMalloc(&b->d_errlog, b->errlog_len * sizeof(float));
+        if (e == cudaSuccess) e = cudaMemset(b->d_errlog, 0, b->errlog_len * sizeof(float));
+    }
+    if (e != cudaSuccess) {
+        destroy_batch(b);
+        return fail(LLG_E_CUDA, "CUDA: %s", cudaGetErrorString(e));
+    }
+    *outb = b;
+    return LLG_OK;
+}
+
+int launch_batch(llg_batch* b, cudaStream_t caller) {
+    for (const Group& g : b->groups)
+        for (const Item& it : g.items) {
+            b->out[it.idx].seconds = 0.0;
+            b->out[it.idx].max_err = 0.0;
+        }
+    CK(cudaEventRecord(b->fork, caller));
+    for (Group& g : b->groups) {
+        int rc = launch_group(b, g, caller);
+        if (rc) return rc;
+    }
+    CK(cudaEventRecord(b->joined, caller));
+    b->launched = true;
+    return LLG_OK;
+}
+
+// Collects every group; round-off aborts are rerun (synchronously) at longer lengths until done.
+int collect_batch(llg_batch* b) {
+    if (b->collected) return LLG_OK;
+    std::vector<Item> retry;
+    for (Group& g : b->groups) {
+        int rc = collect_group(b, g, retry);
+        if (rc) return rc;
+    }
+    for (int round = 0; !retry.empty() && round < 16; ++round) {
+        std::map<uint32_t, std::vector<Item>> byn;
+        for (Item& it : retry) byn[it.n].push_back(it);
+        retry.clear();
+        for (auto& kv : byn) {
+            Group g;
+            g.n = kv.first;
+            g.items = std::move(kv.second);
+            int rc = setup_group(g);
+            if (!rc) {
+                CK(cudaEventRecord(b->fork, g.st));
+                rc = launch_group(b, g, g.st);
+            }
+            if (!rc) rc = collect_group(b, g, retry);
+            release_group(g);
+            if (rc) return rc;
+        }
+    }
+    b->collected = true;
+    return LLG_OK;
+}
+
+cudaStream_t default_stream_for_thread() {
+    static thread_local cudaStream_t st = nullptr;
+    static thread_local int dev = -1;
+    int d = -1;
+    cudaGetDevice(&d);
+    if (!st || dev != d) {
+        cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        dev = d;
+    }
+    return st;
+}
+
+int run_sync(llg_batch* b) {
+    cudaStream_t st = default_stream_for_thread();
+    int rc = launch_batch(b, st);
+    if (rc) return rc;
+    return collect_batch(b);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* llg_status_string(int s) {
+    switch (s) {
+        case LLG_OK: return "ok";
+        case LLG_E_CUDA: return "CUDA error";
+        case LLG_E_NODEV: return "no CUDA device";
+        case LLG_E_ARG: return "invalid argument";
+        case LLG_E_UNSUPPORTED: return "unsupported exponent or length";
+        case LLG_E_ROUNDOFF: return "round-off above threshold at every length";
+        case LLG_E_TIMEOUT: return "device wait timed out";
+        case LLG_E_NOMEM: return "device out of memory";
+        default: return "unknown status";
+    }
+}
+
+const char* llg_last_error(void) { return t_last_error.c_str(); }
+
+int llg_device_info(char* name, size_t cap, int* sms, uint64_t* mem) {
+    int dev;
+    int rc = device_ready(&dev);
+    if (rc) return rc;
+    cudaDeviceProp pr;
+    CK(cudaGetDeviceProperties(&pr, dev));
+    if (name && cap) {
+        std::strncpy(name, pr.name, cap - 1);
+        name[cap - 1] = 0;
+    }
+    if (sms) *sms = pr.multiProcessorCount;
+    if (mem) *mem = (uint64_t)pr.totalGlobalMem;
+    return LLG_OK;
+}
+
+uint32_t llg_fft_length(uint64_t p, double max_bpw) {
+    if (max_bpw <= 0) max_bpw = g_max_bpw;
+    if (p < kWordMaxP) return 0;
+    return fp64_length(p, max_bpw);
+}
+
+int llg_set_max_bpw(double b) {
+    if (!(b >= 2.0 && b <= (double)kMaxDigitBits)) return fail(LLG_E_ARG, "bits per word %g out of range [2, 28]", b);
+    g_max_bpw = b;
+    return LLG_OK;
+}
+
+double llg_get_max_bpw(void) { return g_max_bpw; }
+
+uint32_t llg_ntt_length(uint64_t p) {
+    (void)p;
+    return 0;
+}
+
+uint64_t llg_max_exponent(int engine) {
+    if (engine == LLG_ENGINE_FP64) return (uint64_t)std::floor(g_max_bpw * (double)(1u << kSmallLogMax));
+    return 0;
+}
+
+int llg_run(uint64_t p, uint64_t max_iters, int engine, uint32_t n, llg_result* out,
+            uint64_t* words, size_t nwords) {
+    if (!out) return fail(LLG_E_ARG, "null result pointer");
+    const size_t nw = (size_t)((p + 63) / 64);
+    if (words && nwords < nw) return fail(LLG_E_ARG, "words buffer too small (%zu < %zu)", nwords, nw);
+    llg_batch* b = nullptr;
+    int rc = make_batch(&p, 1, max_iters, engine, n, true, words ? LLG_BATCH_KEEP_WORDS : 0, &b);
+    if (rc) return rc;
+    rc = run_sync(b);
+    if (!rc) rc = llg_batch_results(b, out, words, nwords);
+    destroy_batch(b);
+    if (rc) return rc;
+    return out->status;
+}
+
+int llg_run_batch(const uint64_t* ps, size_t count, uint64_t max_iters, int engine,
+                  llg_result* out, uint64_t* words_out, size_t words_cap) {
+    if (!out || (!ps && count)) return fail(LLG_E_ARG, "null pointer");
+    if (count == 0) return LLG_OK;
+    llg_batch* b = nullptr;
+    int rc = make_batch(ps, count, max_iters, engine, 0, false, words_out ? LLG_BATCH_KEEP_WORDS : 0, &b);
+    if (rc) return rc;
+    rc = run_sync(b);
+    if (!rc) rc = llg_batch_results(b, out, words_out, words_cap);
+    destroy_batch(b);
+    return rc;
+}
+
+int llg_batch_create(const uint64_t* ps, size_t count, uint64_t max_iters, int engine, int flags,
+                     llg_batch** out) {
+    if (!out || !ps || count == 0) return fail(LLG_E_ARG, "null pointer or empty batch");
+    *out = nullptr;
+    return make_batch(ps, count, max_iters, engine, 0, false, flags, out);
+}
+
+int llg_batch_launch(llg_batch* b, void* stream) {
+    if (!b) return fail(LLG_E_ARG, "null batch");
+    cudaStream_t st = stream ? (cudaStream_t)stream : default_stream_for_thread();
+    b->collected = false;
+    return launch_batch(b, st);
+}
+
+int llg_batch_results(llg_batch* b, llg_result* out, uint64_t* words, size_t words_cap) {
+    if (!b || !out) return fail(LLG_E_ARG, "null pointer");
+    if (!b->launched) return fail(LLG_E_ARG, "batch not launched");
+    int rc = collect_batch(b);
+    if (rc) return rc;
+    std::memcpy(out, b->out.data(), b->count * sizeof(llg_result));
+    if (words) {
+        size_t total = 0;
+        for (size_t i = 0; i < b->count; ++i) total += (size_t)((b->ps[i] + 63) / 64);
+        if (words_cap < total) return fail(LLG_E_ARG, "words buffer too small (%zu < %zu)", words_cap, total);
+        if (!b->keep_words) return fail(LLG_E_ARG, "batch created without LLG_BATCH_KEEP_WORDS");
+        std::memset(words, 0, words_cap * sizeof(uint64_t));
+        size_t off = 0;
+        for (size_t i = 0; i < b->count; ++i) {
+            const size_t nw = (size_t)((b->ps[i] + 63) / 64);
+            const std::vector<uint64_t>& w = b->words[i];
+            std::memcpy(words + off, w.data(), std::min(nw, w.size()) * sizeof(uint64_t));
+            off += nw;
+        }
+    }
+    return LLG_OK;
+}
+
+int llg_batch_errlog(llg_batch* b, float* log, size_t cap, size_t* len) {
+    if (!b || !log) return fail(LLG_E_ARG, "null pointer");
+    if (!b->d_errlog) return fail(LLG_E_ARG, "batch created without LLG_BATCH_ERRLOG (single exponent)");
+    const size_t n = std::min(cap, (size_t)b->errlog_len);
+    CK(cudaMemcpy(log, b->d_errlog, n * sizeof(float), cudaMemcpyDeviceToHost));
+    if (len) *len = n;
+    return LLG_OK;
+}
+
+int llg_batch_device_ms(llg_batch* b, float* ms) {
+    if (!b || !ms) return fail(LLG_E_ARG, "null pointer");
+    if (!b->launched) return fail(LLG_E_ARG, "batch not launched");
+    CK(cudaEventSynchronize(b->joined));
+    CK(cudaEventElapsedTime(ms, b->fork, b->joined));
+    return LLG_OK;
+}
+
+void llg_batch_destroy(llg_batch* b) { destroy_batch(b); }
+
+}  // extern "C"

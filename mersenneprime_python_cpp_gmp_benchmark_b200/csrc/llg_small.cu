@@ -1,0 +1,507 @@
+// Whole-test-on-chip FP64 IBDWT Lucas-Lehmer kernel for transform lengths N = 32 .. 8192.
+//
+// One thread block owns one exponent and runs all of its squarings without leaving the SM: the
+// residue lives in registers between iterations and shared memory is only the exchange buffer of
+// the radix passes. This replaces, for small p, the reference's per-test loop of
+// lucaslehmer.cpp:281-311 (FFTW r2c -> square -> c2r -> unweight/round -> carry) and the
+// single-block GPU loop of cuda/ll_ntt.cu:91-163, with a different transform:
+//
+//   * the N real weighted digits are packed as M = N/2 complex values u_m = y_2m + i y_2m+1 and
+//     transformed by an M-point complex FFT (radix-16 passes, in-register DFTs, one shared-memory
+//     exchange per pass, no bit reversal);
+//   * the real-FFT split and the pointwise square are one step on the pair (k, M-k):
+//       U'_k = [(3A - B)(A + B) - w^k (A - B)^2] / 4,  A = U_k, B = conj(U_{M-k}), w = e^{-2 pi i/M}
+//     which equals DFT_M(z_even + i z_odd) for the cyclic square z = y * y;
+//   * the inverse FFT retraces the passes (decimation in time) back to natural order, where each
+//     thread holds u_m for m = t + T*i: unweight, round (1.5*2^52 shifter), max round-off,
+//     balanced carry and re-weighting happen in registers. The carry chain m -> m+1 crosses from
+//     thread t to t+1 (warp shuffle, one shared-memory hop per warp boundary); a thread's carry-out
+//     does not depend on its carry-in (the incoming carry is folded into the first digit and its
+//     small overflow left in the second), so one exchange per iteration suffices and the digits
+//     stay balanced to within a few units.
+//
+// Round-off guard: every iteration's max |x - round(x)| is reduced into the block barrier of the
+// carry exchange; above `abort_err` the test stops with status LLG_ST_ROUNDOFF and the host redoes
+// it at the next larger N.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "llg_device.cuh"
+#include "llg_internal.h"
+
+namespace llg {
+
+template <int LOG_M>
+struct SmallGeom {
+    static constexpr int M = 1 << LOG_M;
+    static constexpr int N = 2 * M;
+    static constexpr int E = 16;               // complex values per thread
+    static constexpr int T = M / E;            // threads per test
+    static constexpr int P = (LOG_M + 3) / 4;  // radix passes
+    static constexpr int RLAST = (LOG_M % 4 == 0) ? 16 : (1 << (LOG_M % 4));
+    static constexpr int PAD = M + M / 16;     // padded exchange array length (doubles)
+    static constexpr int W = (T + 31) / 32;    // warps
+    static __host__ __device__ constexpr int radix(int s) { return s == P - 1 ? RLAST : 16; }
+    static __host__ __device__ constexpr int len(int s) { return M >> (4 * s); }
+    static __host__ __device__ constexpr int stride(int s) { return len(s) / radix(s); }
+};
+
+__device__ __forceinline__ int phys(int x) { return x + (x >> 4); }
+
+// Frequency index k of DIF output position pos (mixed radix 16,...,16,RLAST digit reversal).
+template <class G>
+__device__ __forceinline__ int freq_of_pos(int pos) {
+    int klast = pos % G::RLAST;
+    int rest = pos / G::RLAST;
+    int k = 0;
+#pragma unroll
+    for (int s = 0; s < G::P - 1; ++s) {
+        k = (k << 4) | (rest & 15);
+        rest >>= 4;
+    }
+    // rest digits were stored most-significant-first as k1^(0); the loop above reversed them
+    return k + klast * (G::M / G::RLAST);
+}
+
+template <class G>
+__device__ __forceinline__ int pos_of_freq(int k) {
+    const int klast = k / (G::M / G::RLAST);
+    int low = k % (G::M / G::RLAST);
+    int rest = 0;
+#pragma unroll
+    for (int s = 0; s < G::P - 1; ++s) {
+        rest = (rest << 4) | (low & 15);
+        low >>= 4;
+    }
+    return rest * G::RLAST + klast;
+}
+
+// Forward (INV=false) or inverse radix pass S on the register array v (E values).
+// Forward: load (S > 0), DFT, twiddle w_L^{n2 k1}, store (S < P-1).
+// Inverse: load (S < P-1), conj twiddle, inverse DFT, store (S > 0).
+template <class G, int S, bool INV, bool SYNC_BEFORE_STORE = false>
+__device__ __forceinline__ void radix_pass(double2 (&v)[G::E], double* __restrict__ sre,
+                                           double* __restrict__ sim,
+                                           const double2* __restrict__ qtw, int t) {
+    constexpr int R = G::radix(S);
+    constexpr int L = G::len(S);
+    constexpr int ST = G::stride(S);
+    constexpr int B = G::E / R;
+    constexpr bool LOAD = INV ? (S < G::P - 1) : (S > 0);
+    constexpr bool STORE = INV ? (S > 0) : (S < G::P - 1);
+#pragma unroll
+    for (int h = 0; h < B; ++h) {
+        const int beta = t * B + h;
+        const int g = beta / ST, n2 = beta % ST;
+        const int base = g * L + n2;
+        double2* vv = v + h * R;
+        if constexpr (LOAD) {
+#pragma unroll
+            for (int n1 = 0; n1 < R; ++n1) {
+                const int x = phys(base + n1 * ST);
+                vv[n1] = make_double2(sre[x], sim[x]);
+            }
+        }
+        if constexpr (!INV) {
+            Dft<R, false>::run(vv);
+            if constexpr (ST > 1) {
+#pragma unroll
+                for (int k1 = 1; k1 < R; ++k1)
+                    vv[k1] = cmul(vv[k1], twiddle<G::LOG_M_>(qtw, (uint32_t)(n2 * k1) << (4 * S), false));
+            }
+        } else {
+            if constexpr (ST > 1) {
+#pragma unroll
+                for (int k1 = 1; k1 < R; ++k1)
+                    vv[k1] = cmul(vv[k1], twiddle<G::LOG_M_>(qtw, (uint32_t)(n2 * k1) << (4 * S), true));
+            }
+            Dft<R, true>::run(vv);
+        }
+        if constexpr (STORE && !SYNC_BEFORE_STORE) {
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1) {
+                const int x = phys(base + k1 * ST);
+                sre[x] = vv[k1].x;
+                sim[x] = vv[k1].y;
+            }
+        }
+    }
+    if constexpr (STORE && SYNC_BEFORE_STORE) {
+        __syncthreads();
+#pragma unroll
+        for (int h = 0; h < B; ++h) {
+            const int beta = t * B + h;
+            const int g = beta / ST, n2 = beta % ST;
+            const int base = g * L + n2;
+#pragma unroll
+            for (int k1 = 0; k1 < R; ++k1) {
+                const int x = phys(base + k1 * ST);
+                sre[x] = v[h * R + k1].x;
+                sim[x] = v[h * R + k1].y;
+            }
+        }
+    }
+}
+
+template <class G, int S>
+__device__ __forceinline__ void forward_from(double2 (&v)[G::E], double* sre, double* sim,
+                                             const double2* qtw, int t) {
+    if constexpr (S < G::P) {
+        radix_pass<G, S, false>(v, sre, sim, qtw, t);
+        if constexpr (S < G::P - 1) __syncthreads();
+        forward_from<G, S + 1>(v, sre, sim, qtw, t);
+    }
+}
+
+template <class G, int S>
+__device__ __forceinline__ void inverse_from(double2 (&v)[G::E], double* sre, double* sim,
+                                             const double2* qtw, int t) {
+    if constexpr (S >= 0) {
+        radix_pass<G, S, true, S == G::P - 1>(v, sre, sim, qtw, t);
+        if constexpr (S > 0) __syncthreads();
+        inverse_from<G, S - 1>(v, sre, sim, qtw, t);
+    }
+}
+
+template <int LOG_M_T>
+struct SmallG : SmallGeom<LOG_M_T> {
+    static constexpr int LOG_M_ = LOG_M_T;
+};
+
+template <int LOG_M>
+__global__ void __launch_bounds__(SmallGeom<LOG_M>::T, (SmallGeom<LOG_M>::T < 32 ? 16 : 512 / SmallGeom<LOG_M>::T))
+    ll_small_fp64(const SmallJob* __restrict__ jobs, const double2* __restrict__ qtw_g,
+                  int64_t* __restrict__ digits_out, SmallResult* __restrict__ results,
+                  float* __restrict__ errlog, double abort_err) {
+    using G = SmallG<LOG_M>;
+    constexpr int M = G::M, N = G::N, E = G::E, T = G::T, W = G::W;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* sre = reinterpret_cast<double*>(smem_raw);
+    double* sim = sre + G::PAD;
+    double2* qtw = reinterpret_cast<double2*>(sim + G::PAD);     // M/4 entries
+    double* wB = reinterpret_cast<double*>(qtw + (M / 4 > 0 ? M / 4 : 1));
+    double* iwB = wB + E;
+    int* sB = reinterpret_cast<int*>(iwB + E);
+    long long* cbuf = reinterpret_cast<long long*>(sB + E + (E & 1 ? 1 : 0) + 2);  // W * E
+    unsigned long long* serr = reinterpret_cast<unsigned long long*>(cbuf + W * E);  // 2
+
+    const int t = threadIdx.x;  // blockDim.x == T (a partial warp when T < 32)
+    constexpr bool active = true;
+    unsigned long long t_start = 0;
+    if (t == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_start));
+    const SmallJob job = jobs[blockIdx.x];
+    const uint64_t p = job.p;
+    const uint64_t iters = job.iters;
+    const int q = (int)(p >> (LOG_M + 1));          // p / N
+    const int rem = (int)(p & (uint64_t)(N - 1));   // p % N
+
+    for (int k = t; k < M / 4; k += blockDim.x) qtw[k] = qtw_g[k];
+    for (int i = t; i < E; i += T) {
+        // digit j = 2m + e with m = t + T*i: s_j = (sA(t,e) + sB(i)) mod N
+        const uint64_t s = (uint64_t)(N - (int)(((uint64_t)2 * T * i * p) & (uint64_t)(N - 1))) &
+                           (uint64_t)(N - 1);
+        sB[i] = (int)s;
+        wB[i] = exp2((double)s / (double)N);
+        iwB[i] = exp2(-(double)s / (double)N) / (4.0 * (double)M);
+    }
+    for (int i = t; i < 2; i += T) serr[i] = 0ull;
+    __syncthreads();
+
+    // per-thread weight halves for the even (e=0) and odd (e=1) digit of each u_m
+    int sA0 = 0, sA1 = 0;
+    double wA0 = 1, wA1 = 1, iwA0 = 1, iwA1 = 1;
+    if (active) {
+        sA0 = (int)((uint64_t)(N - (int)(((uint64_t)(2 * t) * p) & (uint64_t)(N - 1))) & (uint64_t)(N - 1));
+        sA1 = (int)((uint64_t)(N - (int)(((uint64_t)(2 * t + 1) * p) & (uint64_t)(N - 1))) & (uint64_t)(N - 1));
+        wA0 = exp2((double)sA0 / (double)N);
+        wA1 = exp2((double)sA1 / (double)N);
+        iwA0 = exp2(-(double)sA0 / (double)N);
+        iwA1 = exp2(-(double)sA1 / (double)N);
+    }
+
+    double2 v[E];
+    // s_0 = 4: digit 0 (thread 0, i = 0, even) has weight a_0 = 1
+#pragma unroll
+    for (int i = 0; i < E; ++i) v[i] = make_double2(0.0, 0.0);
+    if (t == 0) v[0].x = 4.0;
+
+    const int lane = t & 31, warp = t >> 5;
+    const int lastlane = (warp == W - 1) ? ((T - 1) & 31) : 31;
+    const unsigned wmask = (T >= 32) ? 0xffffffffu : ((1u << T) - 1u);
+    double maxerr = 0.0;
+    uint64_t it = 0;
+    uint32_t status = LLG_ST_OK;
+    int x0s[E], x1s[E];
+
+    for (;;) {
+        forward_from<G, 0>(v, sre, sim, qtw, t);
+        // pair (k, M-k): real-FFT split + square, result scaled by 4 (folded into iwB)
+        if (active) {
+#pragma unroll
+            for (int j = 0; j < E; ++j) {
+                const int x = phys(t * E + j);
+                sre[x] = v[j].x;
+                sim[x] = v[j].y;
+            }
+        }
+        __syncthreads();
+        if (active) {
+#pragma unroll
+            for (int j = 0; j < E; ++j) {
+                const int k = freq_of_pos<G>(t * E + j);
+                const int kp = (M - k) & (M - 1);
+                const int x = phys(pos_of_freq<G>(kp));
+                const double2 A = v[j], Bc = make_double2(sre[x], -sim[x]);  // conj(U_{M-k})
+                const double2 s = cadd(A, Bc), d = csub(A, Bc);
+                const double2 a3 = make_double2(3.0 * A.x - Bc.x, 3.0 * A.y - Bc.y);
+                const double2 d2 = make_double2((d.x - d.y) * (d.x + d.y), 2.0 * d.x * d.y);
+                const double2 w = twiddle<LOG_M>(qtw, (uint32_t)k, false);
+                v[j] = csub(cmul(a3, s), cmul(w, d2));
+            }
+            // the first inverse pass stores only after a barrier (partners may still be reading)
+            inverse_from<G, G::P - 1>(v, sre, sim, qtw, t);
+        }
+
+        // unweight, round, error, local carry (even -> odd digit); the carry-out of column i goes
+        // to thread t+1 (lane shuffle) or, at a warp boundary, through cbuf after the barrier
+        double lerr = 0.0;
+        if (active) {
+#pragma unroll
+            for (int i = 0; i < E; ++i) {
+                const int sb = sB[i];
+                const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
+                const int s0 = o0 ? sA0 + sb - N : sA0 + sb;
+                const int s1 = o1 ? sA1 + sb - N : sA1 + sb;
+                const double iw = iwB[i];
+                const double a = v[i].x * (iwA0 * iw) * (o0 ? 2.0 : 1.0);
+                const double b = v[i].y * (iwA1 * iw) * (o1 ? 2.0 : 1.0);
+                long long la, lb;
+                const double ra = round_shift(a, la), rb = round_shift(b, lb);
+                lerr = fmax(lerr, fmax(fabs(a - ra), fabs(b - rb)));
+                const int b0 = q + (s0 < rem), b1 = q + (s1 < rem);
+                long long c;
+                long long x0 = balance(la, b0, c);
+                const long long x1 = balance(lb + c, b1, c);
+                const long long cout = c;
+                if (lane == lastlane) cbuf[warp * E + i] = cout;
+                const long long cin = __shfl_up_sync(wmask, cout, 1);
+                if (lane != 0) {
+                    x0 = balance(x0 + cin, b0, c);
+                    x1s[i] = (int)(x1 + c);
+                } else {
+                    x1s[i] = (int)x1;
+                }
+                x0s[i] = (int)x0;
+            }
+        }
+        maxerr = fmax(maxerr, lerr);
+        if (errlog) atomicMax(&serr[it & 1], (unsigned long long)__double_as_longlong(lerr));
+        const int bad = __syncthreads_or(lerr > abort_err);
+        if (errlog && t == 0) {
+            errlog[it] = (float)__longlong_as_double((long long)serr[it & 1]);
+            serr[(it + 1) & 1] = 0ull;
+        }
+        if (active && lane == 0) {
+#pragma unroll
+            for (int i = 0; i < E; ++i) {
+                long long cin = (warp > 0) ? cbuf[(warp - 1) * E + i]
+                                           : cbuf[(W - 1) * E + ((i + E - 1) % E)];  // m-1 wraps at m=0
+                if (t == 0 && i == 0) cin -= 2;  // the "- 2" of s^2 - 2
+                const int sb = sB[i];
+                const bool o0 = sA0 + sb >= N;
+                const int s0 = o0 ? sA0 + sb - N : sA0 + sb;
+                const int b0 = q + (s0 < rem);
+                long long c;
+                const long long x0 = balance((long long)x0s[i] + cin, b0, c);
+                x0s[i] = (int)x0;
+                x1s[i] = (int)((long long)x1s[i] + c);
+            }
+        }
+        ++it;
+        if (bad) {
+            status = LLG_ST_ROUNDOFF;
+            break;
+        }
+        if (it >= iters) break;
+        if (active) {
+#pragma unroll
+            for (int i = 0; i < E; ++i) {
+                const int sb = sB[i];
+                const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
+                const double w = wB[i];
+                v[i].x = i2d_shift(x0s[i]) * (wA0 * w) * (o0 ? 0.5 : 1.0);
+                v[i].y = i2d_shift(x1s[i]) * (wA1 * w) * (o1 ? 0.5 : 1.0);
+            }
+        }
+    }
+
+    if (active && digits_out) {
+        int64_t* out = digits_out + (size_t)blockIdx.x * N;
+#pragma unroll
+        for (int i = 0; i < E; ++i) {
+            const int m = t + T * i;
+            out[2 * m] = x0s[i];
+            out[2 * m + 1] = x1s[i];
+        }
+    }
+    // block max of the round-off (non-negative doubles order like their bit patterns)
+    __syncthreads();
+    if (t == 0) serr[0] = 0ull;
+    __syncthreads();
+    atomicMax(&serr[0], (unsigned long long)__double_as_longlong(maxerr));
+    __syncthreads();
+    if (t == 0) {
+        SmallResult r;
+        r.max_err = __longlong_as_double((long long)serr[0]);
+        r.iters_done = it;
+        r.status = status;
+        unsigned long long t_end;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_end));
+        r.ns = t_end - t_start;
+        results[blockIdx.x] = r;
+    }
+}
+
+// p < 256: s <- s^2 - 2 mod 2^p - 1 on four 64-bit limbs (schoolbook square, shift-and-add
+// reduction as in lucaslehmer.cpp:42-48), one thread per exponent. Exact; used where digits of
+// an FFT length would hold too few bits for a stable balanced carry.
+__device__ __forceinline__ void word_reduce(uint64_t (&s)[4], const uint64_t (&w)[8], int p) {
+    // lo = w mod 2^p, hi = w >> p, s = lo + hi (both < 2^p), then conditional subtract of M
+    uint64_t lo[4], hi[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int bit = 64 * i;
+        lo[i] = (bit + 64 <= p) ? w[i] : (bit < p ? (w[i] & ((1ull << (p - bit)) - 1ull)) : 0ull);
+        // hi limb i = bits [p + 64 i, p + 64 i + 64)
+        const int q = (p + bit) >> 6, r = (p + bit) & 63;
+        const uint64_t a0 = q < 8 ? w[q] : 0ull, a1 = q + 1 < 8 ? w[q + 1] : 0ull;
+        hi[i] = r ? ((a0 >> r) | (a1 << (64 - r))) : a0;
+    }
+    unsigned __int128 c = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        c += (unsigned __int128)lo[i] + hi[i];
+        s[i] = (uint64_t)c;
+        c >>= 64;
+    }
+    // s < 2^(p+1): fold bit p back (2^p == 1) until s < 2^p, then s == M -> 0
+    for (int guard = 0; guard < 3; ++guard) {
+        const int q = p >> 6, r = p & 63;
+        const uint64_t top = (q < 4) ? (s[q] >> r) : 0ull;
+        if (!top) break;
+        if (q < 4) s[q] &= (r ? ((1ull << r) - 1ull) : 0ull);
+        unsigned __int128 cc = top;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            cc += s[i];
+            s[i] = (uint64_t)cc;
+            cc >>= 64;
+        }
+    }
+    bool all = true;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int bit = 64 * i;
+        const uint64_t full = (bit + 64 <= p) ? ~0ull : (bit < p ? ((1ull << (p - bit)) - 1ull) : 0ull);
+        all = all && (s[i] == full);
+    }
+    if (all)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) s[i] = 0ull;
+}
+
+__global__ void ll_word(const SmallJob* __restrict__ jobs, int n, uint64_t* __restrict__ res) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int p = (int)jobs[i].p;
+    const uint64_t iters = jobs[i].iters;
+    uint64_t s[4] = {4ull, 0ull, 0ull, 0ull};
+    if (p == 2) s[0] = 1ull;  // 4 mod 3
+    for (uint64_t k = 0; k < iters; ++k) {
+        uint64_t w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            unsigned __int128 c = 0;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                c += (unsigned __int128)s[a] * s[b] + w[a + b];
+                w[a + b] = (uint64_t)c;
+                c >>= 64;
+            }
+            w[a + 4] = (uint64_t)c;
+        }
+        word_reduce(s, w, p);
+        // s - 2 mod M
+        if (s[0] >= 2 || s[1] || s[2] || s[3]) {
+            unsigned __int128 b = 2;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint64_t x = s[j];
+                s[j] = x - (uint64_t)b;
+                b = (x < (uint64_t)b) ? 1 : 0;
+            }
+        } else {  // s in {0, 1}: s - 2 + M = M - (2 - s)
+            const uint64_t v = s[0];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int bit = 64 * j;
+                s[j] = (bit + 64 <= p) ? ~0ull : (bit < p ? ((1ull << (p - bit)) - 1ull) : 0ull);
+            }
+            s[0] -= 2ull - v;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) res[(size_t)i * 4 + j] = s[j];
+}
+
+cudaError_t launch_word(const SmallJob* jobs, int njobs, uint64_t* res, cudaStream_t st) {
+    ll_word<<<(njobs + 127) / 128, 128, 0, st>>>(jobs, njobs, res);
+    return cudaGetLastError();
+}
+
+template <int LOG_M>
+static size_t small_smem_bytes() {
+    using G = SmallGeom<LOG_M>;
+    size_t b = 2 * sizeof(double) * G::PAD;
+    b += sizeof(double2) * (G::M / 4 > 0 ? G::M / 4 : 1);
+    b += 2 * sizeof(double) * G::E + sizeof(int) * (G::E + (G::E & 1 ? 1 : 0) + 2);
+    b += sizeof(long long) * G::W * G::E + 2 * sizeof(unsigned long long);
+    return b;
+}
+
+template <int LOG_M>
+static cudaError_t launch_small_t(const SmallJob* jobs, int njobs, const double2* qtw,
+                                  int64_t* digits, SmallResult* results, float* errlog,
+                                  double abort_err, cudaStream_t st) {
+    using G = SmallGeom<LOG_M>;
+    const size_t smem = small_smem_bytes<LOG_M>();
+    static bool configured = false;  // benign race: the attribute call is idempotent
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(ll_small_fp64<LOG_M>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    ll_small_fp64<LOG_M><<<njobs, G::T, smem, st>>>(jobs, qtw, digits, results, errlog, abort_err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_small_fp64(int log_n, const SmallJob* jobs, int njobs, const double2* qtw,
+                              int64_t* digits, SmallResult* results, float* errlog,
+                              double abort_err, cudaStream_t st) {
+    switch (log_n - 1) {
+        case 4: return launch_small_t<4>(jobs, njobs, qtw, digits, results, errlog, abort_err, st);
+        case 5: return launch_small_t<5>(jobs, njobs, qtw, digits, results, errlog, abort_err, st);
+        case 6: return launch_small_t<6>(jobs, njobs, qtw, digits, results, errlog, abort_err, st);
+        case 7: return launch_small_t<7>(jobs, njobs, qtw, digits, results, errlog, abort_err, st);
+        case 8: return launch_small_t<8>(jobs, njobs, qtw, digits, results, errlog, abort_err, st);
+        case 9: return launch_small_t<9>(jobs, njobs, qtw, digits, results, errlog, abort_err, st);
+        case 10: return launch_small_t<10>(jobs, njobs, qtw, digits, results, errlog, abort_err, st);
+        case 11: return launch_small_t<11>(jobs, njobs, qtw, digits, results, errlog, abort_err, st);
+        case 12: return launch_small_t<12>(jobs, njobs, qtw, digits, results, errlog, abort_err, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace llg

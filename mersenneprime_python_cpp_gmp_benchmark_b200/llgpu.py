@@ -1,0 +1,198 @@
+"""ctypes binding of the C-ABI in include/llgpu.h (libllgpu.so, built in-tree).
+
+This is the reference-side binding a Python caller would add for the boundary (the pybind11
+modules in this package bind the same entry points for the reference's module surface). Loading
+fails loudly when libllgpu.so is missing: there is no CPU path behind it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+from . import LIB_PATH, PKG_DIR
+
+HEADER = os.path.join(os.path.dirname(PKG_DIR), "include", "llgpu.h")
+
+ENGINES = {"fp64": 0, "ntt": 1}
+STATUS = {0: "LLG_OK", 1: "LLG_E_CUDA", 2: "LLG_E_NODEV", 3: "LLG_E_ARG", 4: "LLG_E_UNSUPPORTED",
+          5: "LLG_E_ROUNDOFF", 6: "LLG_E_TIMEOUT", 7: "LLG_E_NOMEM"}
+
+
+class LlgResult(ctypes.Structure):
+    _fields_ = [("p", ctypes.c_uint64), ("iters", ctypes.c_uint64), ("res64", ctypes.c_uint64),
+                ("max_err", ctypes.c_double), ("seconds", ctypes.c_double), ("n", ctypes.c_uint32),
+                ("escalations", ctypes.c_uint32), ("is_zero", ctypes.c_int32), ("status", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class LlgError(RuntimeError):
+    def __init__(self, code, detail=""):
+        self.code = code
+        super().__init__(f"{STATUS.get(code, code)}: {detail}")
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built; run mersenneprime_python_cpp_gmp_benchmark_b200.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        u64, u32, i32, dbl, sz = ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int32, ctypes.c_double, ctypes.c_size_t
+        P = ctypes.POINTER
+        L.llg_status_string.argtypes = [ctypes.c_int]
+        L.llg_status_string.restype = ctypes.c_char_p
+        L.llg_last_error.argtypes = []
+        L.llg_last_error.restype = ctypes.c_char_p
+        L.llg_device_info.argtypes = [ctypes.c_char_p, sz, P(ctypes.c_int), P(u64)]
+        L.llg_fft_length.argtypes = [u64, dbl]
+        L.llg_fft_length.restype = u32
+        L.llg_set_max_bpw.argtypes = [dbl]
+        L.llg_get_max_bpw.restype = dbl
+        L.llg_ntt_length.argtypes = [u64]
+        L.llg_ntt_length.restype = u32
+        L.llg_max_exponent.argtypes = [ctypes.c_int]
+        L.llg_max_exponent.restype = u64
+        L.llg_run.argtypes = [u64, u64, ctypes.c_int, u32, P(LlgResult), P(u64), sz]
+        L.llg_run_batch.argtypes = [P(u64), sz, u64, ctypes.c_int, P(LlgResult), P(u64), sz]
+        L.llg_residue_from_digits.argtypes = [u64, u32, P(ctypes.c_int64), P(u64), sz, P(u64), P(i32)]
+        L.llg_batch_create.argtypes = [P(u64), sz, u64, ctypes.c_int, ctypes.c_int, P(ctypes.c_void_p)]
+        L.llg_batch_launch.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.llg_batch_results.argtypes = [ctypes.c_void_p, P(LlgResult), P(u64), sz]
+        L.llg_batch_errlog.argtypes = [ctypes.c_void_p, P(ctypes.c_float), sz, P(sz)]
+        L.llg_measure_peak.argtypes = [ctypes.c_int, P(dbl)]
+        L.llg_batch_device_ms.argtypes = [ctypes.c_void_p, P(ctypes.c_float)]
+        L.llg_batch_destroy.argtypes = [ctypes.c_void_p]
+        L.llg_batch_destroy.restype = None
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise LlgError(rc, (lib().llg_last_error() or b"").decode())
+
+
+def header_functions():
+    """Names of the functions include/llgpu.h declares."""
+    src = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\*?\s*(llg_[a-z_0-9]+)\s*\(", src, re.M)))
+
+
+def nwords(p):
+    return max(1, (p + 63) // 64)
+
+
+def device_info():
+    name = ctypes.create_string_buffer(256)
+    sms, mem = ctypes.c_int(), ctypes.c_uint64()
+    _check(lib().llg_device_info(name, 256, ctypes.byref(sms), ctypes.byref(mem)))
+    return name.value.decode(), sms.value, mem.value
+
+
+def measure_peak(which="fp64"):
+    """Measured ops/s: 'fp64' FMA flops/s or 'int32' multiply-adds/s."""
+    v = ctypes.c_double()
+    _check(lib().llg_measure_peak(0 if which == "fp64" else 1, ctypes.byref(v)))
+    return v.value
+
+
+def fft_length(p, max_bpw=0.0):
+    return int(lib().llg_fft_length(p, max_bpw))
+
+
+def ntt_length(p):
+    return int(lib().llg_ntt_length(p))
+
+
+def run(p, iters=0, engine="fp64", n=0, want_words=False):
+    """One test (or its first `iters` squarings) -> dict of llg_result fields (+ 'words')."""
+    r = LlgResult()
+    words = (ctypes.c_uint64 * nwords(p))() if want_words else None
+    _check(lib().llg_run(p, iters, ENGINES[engine], n, ctypes.byref(r), words, nwords(p) if want_words else 0))
+    d = r.as_dict()
+    if want_words:
+        d["words"] = list(words)
+    return d
+
+
+def run_batch(ps, iters=0, engine="fp64", want_words=False):
+    ps = list(ps)
+    arr = (ctypes.c_uint64 * len(ps))(*ps)
+    out = (LlgResult * len(ps))()
+    total = sum(nwords(p) for p in ps)
+    words = (ctypes.c_uint64 * total)() if want_words else None
+    _check(lib().llg_run_batch(arr, len(ps), iters, ENGINES[engine], out, words, total if want_words else 0))
+    res = [o.as_dict() for o in out]
+    if want_words:
+        off = 0
+        for d, p in zip(res, ps):
+            d["words"] = list(words[off:off + nwords(p)])
+            off += nwords(p)
+    return res
+
+
+class Batch:
+    """A device-resident batch (llg_batch_*): create once, launch on a stream, read results."""
+
+    KEEP_WORDS, ERRLOG = 1, 2
+
+    def __init__(self, ps, iters=0, engine="fp64", flags=0):
+        self.ps = list(ps)
+        arr = (ctypes.c_uint64 * len(self.ps))(*self.ps)
+        self.h = ctypes.c_void_p()
+        self.flags = flags
+        _check(lib().llg_batch_create(arr, len(self.ps), iters, ENGINES[engine], flags, ctypes.byref(self.h)))
+
+    def launch(self, stream=0):
+        """Enqueue on a CUDA stream handle (int, e.g. torch.cuda.Stream.cuda_stream; 0 = internal)."""
+        _check(lib().llg_batch_launch(self.h, ctypes.c_void_p(stream or None)))
+
+    def results(self, want_words=False):
+        out = (LlgResult * len(self.ps))()
+        total = sum(nwords(p) for p in self.ps)
+        words = (ctypes.c_uint64 * total)() if want_words else None
+        _check(lib().llg_batch_results(self.h, out, words, total if want_words else 0))
+        res = [o.as_dict() for o in out]
+        if want_words:
+            off = 0
+            for d, p in zip(res, self.ps):
+                d["words"] = list(words[off:off + nwords(p)])
+                off += nwords(p)
+        return res
+
+    def device_ms(self):
+        ms = ctypes.c_float()
+        _check(lib().llg_batch_device_ms(self.h, ctypes.byref(ms)))
+        return ms.value
+
+    def errlog(self):
+        n = self.ps and max(self.ps) or 0
+        buf = (ctypes.c_float * n)()
+        ln = ctypes.c_size_t()
+        _check(lib().llg_batch_errlog(self.h, buf, n, ctypes.byref(ln)))
+        return list(buf[:ln.value])
+
+    def close(self):
+        if self.h:
+            lib().llg_batch_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def residue_from_digits(p, n, digits):
+    d = (ctypes.c_int64 * n)(*[int(x) for x in digits])
+    words = (ctypes.c_uint64 * nwords(p))()
+    r64, z = ctypes.c_uint64(), ctypes.c_int32()
+    _check(lib().llg_residue_from_digits(p, n, d, words, nwords(p), ctypes.byref(r64), ctypes.byref(z)))
+    return bool(z.value), r64.value, list(words)

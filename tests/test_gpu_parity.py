@@ -1,0 +1,89 @@
+"""Parity of the CUDA path with the oracle, through the C-ABI (libllgpu.so via ctypes).
+
+Bit-exact integer results: full residues (every limb) against the oracle's GMP restatement and
+the committed golden fingerprints; the word path (p < 64); every power-of-two length of the
+whole-test kernel; interim residues; the round-off escalation path."""
+import os
+import random
+
+import pytest
+
+from conftest import GOLDEN, load_range
+
+pytestmark = pytest.mark.gpu
+
+
+def test_word_path_all_small_exponents(gpu, oracle):
+    """p < 256 runs on the exact multi-limb kernel: every exponent, full residue."""
+    for p in range(2, 256):
+        r = gpu.run(p, want_words=True)
+        v, res, words = oracle.ll_gmp(p)
+        assert (bool(r["is_zero"]), r["res64"]) == (v, res), p
+        if p >= 3 and p % 2:
+            assert r["words"] == words
+
+
+@pytest.mark.parametrize("logn", range(5, 14))
+def test_every_length_full_residue(gpu, oracle, logn):
+    n = 1 << logn
+    rng = random.Random(logn)
+    lo = max(256, n * ((logn + 5) // 2))  # the length's bits-per-digit floor
+    ps = [p for p in oracle.primes(lo, min(18 * n, 30000)) if p % 2]
+    for p in rng.sample(ps, min(4, len(ps))):
+        r = gpu.run(p, n=n, want_words=True)
+        v, res, words = oracle.ll_gmp(p)
+        assert r["status"] == 0 and r["n"] == n
+        assert r["words"] == words, (p, n)
+        assert bool(r["is_zero"]) == v and r["max_err"] < 0.4
+
+
+@pytest.mark.parametrize("p,k", [(127, 1), (4423, 2), (9689, 3), (20011, 17), (44497, 1000), (100003, 123)])
+def test_interim_full_residue(gpu, oracle, p, k):
+    r = gpu.run(p, iters=k, want_words=True)
+    assert r["iters"] == k
+    assert r["words"] == oracle.ll_gmp(p, k)[2]
+
+
+def test_all_primes_to_10001_full_residues(gpu, oracle):
+    """Config: every prime p <= 10001 (1229 exponents, 22 hits), full residues bit-exact."""
+    rows = load_range()
+    ps = [p for p in oracle.primes(2, 10001)]
+    out = gpu.run_batch(ps, want_words=True)
+    hits = []
+    for p, r in zip(ps, out):
+        v, res, h = rows[p]
+        assert r["status"] == 0
+        assert (bool(r["is_zero"]), r["res64"], oracle.residue_hash(r["words"])) == (v, res, h), p
+        if r["is_zero"]:
+            hits.append(p)
+    assert len(hits) == 22
+
+
+def test_batch_matches_single(gpu):
+    ps = [1279, 2203, 4421, 9941, 11213, 19937, 21701, 23209]
+    b = gpu.run_batch(ps, iters=500)
+    for p, rb in zip(ps, b):
+        rs = gpu.run(p, iters=500)
+        assert rb["res64"] == rs["res64"] and rb["n"] == rs["n"]
+
+
+def test_roundoff_escalation_stays_exact(gpu, oracle):
+    """Force a length far too short (27 bits per digit: the convolution outgrows FP64's 53 bits):
+    the kernel must abort on round-off, the host must redo it at a longer length on the GPU, and
+    the residue must still be exact."""
+    p = 27611
+    r = gpu.run(p, iters=300, n=1024, want_words=True)
+    assert r["status"] == 0 and r["escalations"] >= 1 and r["n"] > 1024
+    assert r["words"] == oracle.ll_gmp(p, 300)[2]
+
+
+def test_unsupported_exponent_is_an_error(gpu):
+    with pytest.raises(gpu.LlgError):
+        gpu.run(10**12 + 39)
+
+
+def test_trivial_exponents(gpu):
+    assert gpu.run(2)["is_zero"] == 1
+    assert gpu.run(4)["is_zero"] == 0
+    assert gpu.run(1)["is_zero"] == 0
+    assert gpu.run(0)["is_zero"] == 0
