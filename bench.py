@@ -36,6 +36,9 @@ for _p in (ROOT, PKG):
 
 RANGE_HI = 100001
 METRIC_RANGE = "tests/s for all p<=100001 (residues exact)"
+BIG_P = 136279841
+METRIC_BIG = "us/LL-iteration at p=136,279,841"
+STEP_ITERS = 1000  # squarings per timed step of the p=136,279,841 workload
 
 
 def sieve(lo, hi):
@@ -229,8 +232,106 @@ def bench_range(args, rank, world):
                      "work": "5 N log2 N flops per squaring x (p-2) squarings, summed over the range"},
         "clocks": clk.summary(),
         "hits": len(hits),
+        "gpu_launches": args.steps * len({r["n"] for r in res}),
     }
     return line
+
+
+def bench_big(args, rank, world):
+    """p = 136,279,841 on the two-pass engine at N = 2^23; one step = 1000 squarings."""
+    import torch
+    from mersenneprime_python_cpp_gmp_benchmark_b200 import llgpu
+    n = 1 << 23
+    stream = torch.cuda.Stream()
+    handle = stream.cuda_stream
+    t = llgpu.Test(BIG_P, n)
+    t.start(handle)
+    flush = L2Flush()
+    for _ in range(args.warmup):
+        t.iterate(STEP_ITERS, handle)
+    torch.cuda.synchronize()
+    barrier(world)
+    times = []
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        for _ in range(args.steps):
+            flush()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            t.iterate(STEP_ITERS, handle)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1) * 1e-3)
+    torch.cuda.synchronize()
+    barrier(world)
+    done = 1 + STEP_ITERS * (args.warmup + args.steps)
+    r = t.read(handle)
+    assert r["iters"] == done and r["status"] == 0, r
+    t.close()
+    t_rank = sum(times)
+    t_max = max_over_ranks(t_rank, world)
+    us_iter = 1e6 * t_max / (STEP_ITERS * args.steps)
+    # correctness of the timed engine: res64 after 1000 squarings vs the reference GMP engine
+    gold = {(d["p"], d["k"]): int(d["res64"], 16)
+            for d in json.load(open(os.path.join(ROOT, "tests", "golden", "appendix.json")))["after"]}
+    chk = llgpu.run(BIG_P, iters=1000, n=n)
+    assert chk["res64"] == gold[(BIG_P, 1000)], "res64 after 1000 squarings differs from the reference"
+    # e2e: the reference-facing call, host in / host out, for a 2000-squaring interim residue
+    import lucaslehmer as ll
+    k_e2e = 2000
+    t0 = time.perf_counter()
+    res64, err = ll.fft_res64_after(BIG_P, k_e2e)
+    t_e2e = time.perf_counter() - t0
+    t_e2e = max_over_ranks(t_e2e, world)
+    bytes_iter = 32.0 * n   # two read+write sweeps of the 8N-byte state
+    flops_iter = 5.0 * n * 23
+    hbm_peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"] \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
+    achieved = bytes_iter / (us_iter * 1e-6) / 1e9
+    fp64_peak = llgpu.measure_peak("fp64") / 1e12
+    line = {
+        "metric": METRIC_BIG, "value": round(us_iter, 3), "unit": "us/iteration", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * t_max / args.steps, 3),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: the LL sequence of p=136,279,841 from s_0=4 (no external data)",
+        "config": {"workload": "p=136,279,841 FP64 IBDWT, N=2^23 (16.25 bits/digit), two-pass "
+                               "(row 1024 x column 4096), 1000 squarings per step",
+                   "l2": "flushed (512 MiB write) between steps; the 64 MiB state stays on device",
+                   "parallelism": f"one independent test per GPU ({world} replica(s))"},
+        "e2e": {"value": round(1e6 * t_e2e / k_e2e, 3), "unit": "us/iteration", "iters": k_e2e,
+                "call": "lucaslehmer.fft_res64_after(136279841, 2000): tables, s_0 upload, squarings, "
+                        "digits D2H, exact residue rebuild",
+                "h2d_bytes_per_step": 4 * n, "d2h_bytes_per_step": 4 * n},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                     "frac": round(achieved / hbm_peak, 4), "peak_source": "MEASURED_PEAKS.json hbm_gbs",
+                     "traffic": None,
+                     "work": "32 N bytes per squaring (two read+write sweeps of the 8N-byte state)"},
+        "roofline_fp64": {"achieved": round(flops_iter / (us_iter * 1e-6) / 1e12, 3), "peak": round(fp64_peak, 3),
+                          "unit": "TFLOP/s", "frac": round(flops_iter / (us_iter * 1e-6) / 1e12 / fp64_peak, 4),
+                          "work": "5 N log2 N flops per squaring", "peak_source": "measured FP64 FMA probe"},
+        "max_roundoff": r["max_err"],
+        "clocks": clk.summary(),
+        "gpu_launches": 2 * STEP_ITERS * args.steps,
+    }
+    return line
+
+
+def cpu_baseline_big(threads):
+    """Reference GMP engine (oracle/_ref) per-iteration time at p = 136,279,841: one full-size
+    squaring timed as gmp_res64_after(p, 29) - gmp_res64_after(p, 27) (s_k fills p bits by k~27)."""
+    from oracle import oracle
+    ref = oracle.reference_module()
+    kind = "reference" if ref is not None else "port"
+    f = (lambda k: ref.gmp_res64_after(BIG_P, k)) if ref else (lambda k: oracle.ll_gmp(BIG_P, k))
+    t0 = time.perf_counter()
+    f(27)
+    t1 = time.perf_counter()
+    f(30)
+    t2 = time.perf_counter()
+    per = ((t2 - t1) - (t1 - t0)) / 3.0
+    return {"value": round(per * 1e6, 1), "unit": "us/iteration", "cores": 1, "kind": kind,
+            "sample": "reference GMP engine (lucas_lehmer_n via gmp_res64_after), p=136,279,841: "
+                      "(time of 30 squarings - time of 27) / 3, i.e. full-size squarings; one core "
+                      "(the reference's engine is single-threaded per test)"}
 
 
 def cpu_baseline_range(threads, budget_s=20.0):
@@ -264,7 +365,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", choices=("range",), default="range")
+    ap.add_argument("--workload", choices=("big", "range"), default="big")
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -290,11 +391,14 @@ def main():
         print(json.dumps(line))
         return 0
     rank, world, local = dist_setup(args.gpus)
-    line = bench_range(args, rank, world)
+    if args.workload == "range":
+        line = bench_range(args, rank, world)
+    else:
+        line = bench_big(args, rank, world)
     if rank == 0:
         if not args.no_cpu_baseline and world == 1:
-            line["cpu_baseline"] = cpu_baseline_range(threads)
-        line["gpu_launches"] = (args.steps) * 9  # one whole-test launch per length group per step
+            line["cpu_baseline"] = (cpu_baseline_range(threads) if args.workload == "range"
+                                    else cpu_baseline_big(threads))
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist

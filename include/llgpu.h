@@ -108,6 +108,22 @@ int llg_batch_errlog(llg_batch* b, float* log, size_t cap, size_t* len);
 int llg_batch_device_ms(llg_batch* b, float* ms);
 void llg_batch_destroy(llg_batch* b);
 
+/* One exponent's device state on the two-pass engine (lengths 2^14 .. 2^23), for callers that
+ * drive the iterations themselves (interim residues, timing on their own stream):
+ * create (tables, state; n == 0 picks the length), start (s_0 = 4 and the first squaring),
+ * iterate (enqueue squarings as CUDA-graph replays, no host sync), read (final row pass, digits
+ * back, exact residue; waits). llg_result.iters counts the squarings done since start;
+ * llg_result.status is LLG_E_ROUNDOFF when the worst round-off exceeded 0.4 (no escalation here).
+ * llg_test_errlog: per-squaring max round-off (ring of 65536 entries).
+ * Replaces the iteration loop of lucas_lehmer_fft_raw(), lucaslehmer.cpp:281-311, for large p. */
+typedef struct llg_test llg_test;
+int llg_test_create(uint64_t p, uint32_t n, llg_test** out);
+int llg_test_start(llg_test* t, void* stream);
+int llg_test_iterate(llg_test* t, uint64_t iters, void* stream);
+int llg_test_read(llg_test* t, void* stream, llg_result* out, uint64_t* words, size_t nwords);
+int llg_test_errlog(llg_test* t, float* log, size_t cap, size_t* len);
+void llg_test_destroy(llg_test* t);
+
 /* Exact residue of balanced (or any signed) digits: s = sum_j d_j 2^ceil(jp/n) mod 2^p - 1.
  * Host-only; needs no GPU. Replaces the GMP rebuild, lucaslehmer.cpp:312-323 and
  * cuda/ll_ntt.cu:238-252. Returns LLG_OK; *is_zero set when s == 0. */

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/llgpu.h"
+#include "llg_host.h"
 #include "llg_internal.h"
 
 namespace {
@@ -108,15 +109,26 @@ constexpr uint64_t kWordMaxP = 256;     // p below this runs on the exact multi-
 // A length is usable when every digit has enough bits for the one-exchange balanced carry to stay
 // balanced (floor(p/N) >= log2(N)/2 + 2: the carry into a digit is ~sqrt(N) times smaller than its
 // base) and few enough for int32 digits and FP64 products.
+constexpr int kLargeLogMax = 23;
+
+bool is_small_length(uint64_t n) {
+    const int l = ilog2_exact(n);
+    return l >= kSmallLogMin && l <= kSmallLogMax;
+}
+
+// The two-pass engine's three-hop carry keeps digits balanced down to ~log2(N)/4 + 1 bits per
+// digit; it asks for floor(p/N) >= log2(N)/4 + 3.
 bool fp64_length_usable(uint64_t p, uint64_t n) {
     const int l = ilog2_exact(n);
-    if (l < kSmallLogMin || l > kSmallLogMax) return false;
-    return 2 * (p / n) >= (uint64_t)l + 4 && (p + n - 1) / n <= kMaxDigitBits;
+    if ((p + n - 1) / n > kMaxDigitBits) return false;
+    if (is_small_length(n)) return 2 * (p / n) >= (uint64_t)l + 4;
+    if (l > kSmallLogMax && large_length_supported(l)) return 4 * (p / n) >= (uint64_t)l + 12;
+    return false;
 }
 
 // smallest usable length with p / N <= bpw
 uint32_t fp64_length(uint64_t p, double bpw) {
-    for (int l = kSmallLogMin; l <= kSmallLogMax; ++l) {
+    for (int l = kSmallLogMin; l <= kLargeLogMax; ++l) {
         const uint64_t N = 1ull << l;
         if ((double)p / (double)N <= bpw && fp64_length_usable(p, N)) return (uint32_t)N;
     }
@@ -124,7 +136,7 @@ uint32_t fp64_length(uint64_t p, double bpw) {
 }
 
 uint32_t next_fp64_length(uint64_t p, uint32_t n) {
-    for (int l = kSmallLogMin; l <= kSmallLogMax; ++l) {
+    for (int l = kSmallLogMin; l <= kLargeLogMax; ++l) {
         const uint64_t N = 1ull << l;
         if (N > n && fp64_length_usable(p, N)) return (uint32_t)N;
     }
@@ -167,6 +179,7 @@ struct llg_batch {
     std::vector<uint64_t> ps;
     std::vector<llg_result> out;
     std::vector<Group> groups;
+    std::vector<Item> large;      // two-pass engine exponents, run one at a time at collect
     cudaEvent_t fork = nullptr;   // recorded on the caller's stream at launch (timing enabled)
     cudaEvent_t joined = nullptr; // recorded on the caller's stream after every group joined
     bool launched = false;
@@ -303,6 +316,95 @@ int collect_group(llg_batch* b, Group& g, std::vector<Item>& retry) {
     return LLG_OK;
 }
 
+// One exponent on the two-pass engine: chunks of squarings with a round-off check after each;
+// above the threshold the test restarts from s_0 at the next usable length.
+constexpr uint64_t kCheckChunk = 4096;
+constexpr double kAbortErrLarge = 0.4;
+
+double bits_to_double(unsigned long long b) {
+    double d;
+    std::memcpy(&d, &b, sizeof d);
+    return d;
+}
+
+int run_large(const Item& item, llg_result& r, std::vector<uint64_t>* words, cudaStream_t st) {
+    uint32_t n = item.n;
+    uint32_t esc = item.escalations;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    for (;;) {
+        LargeTest T;
+        CK(T.init(item.p, ilog2_exact(n)));
+        CK(cudaEventRecord(e0, st));
+        CK(T.start(seed_digits(n), st));
+        uint64_t left = item.iters - 1;
+        bool abort = false;
+        double worst = 0.0;
+        while (left > 0 && !abort) {
+            const uint64_t k = std::min(left, kCheckChunk);
+            CK(T.step(k, st));
+            left -= k;
+            LargeCtl h;
+            CK(T.read_ctl(h, st));
+            if (h.timeout) {
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                return fail(LLG_E_TIMEOUT, "carry wait timed out (p=%llu)", (unsigned long long)item.p);
+            }
+            worst = bits_to_double(h.err_max);
+            if (worst > kAbortErrLarge) abort = true;
+        }
+        std::vector<int> digits;
+        if (!abort) {
+            CK(T.finish(st, digits));
+            CK(cudaEventRecord(e1, st));
+            LargeCtl h;
+            CK(T.read_ctl(h, st));
+            worst = bits_to_double(h.err_max);
+            if (h.timeout) {
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                return fail(LLG_E_TIMEOUT, "carry wait timed out (p=%llu)", (unsigned long long)item.p);
+            }
+            if (worst > kAbortErrLarge) abort = true;
+        }
+        r.max_err = std::max(r.max_err, worst);
+        if (abort) {
+            const uint32_t nn = next_fp64_length(item.p, n);
+            if (!nn) {
+                r.status = LLG_E_ROUNDOFF;
+                r.n = n;
+                r.escalations = esc;
+                break;
+            }
+            n = nn;
+            ++esc;
+            continue;
+        }
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        std::vector<int64_t> d64(digits.begin(), digits.end());
+        const size_t nw = (size_t)((item.p + 63) / 64);
+        std::vector<uint64_t> w(nw);
+        int32_t z = 0;
+        const int rc = llg_residue_from_digits(item.p, n, d64.data(), w.data(), nw, &r.res64, &z);
+        if (rc) return rc;
+        if (words) *words = std::move(w);
+        r.iters = item.iters;
+        r.is_zero = z;
+        r.n = n;
+        r.escalations = esc;
+        r.seconds = ms * 1e-3;
+        r.max_err = worst;
+        r.status = LLG_OK;
+        break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return LLG_OK;
+}
+
 // Creates a batch: trivial exponents resolved on the host, the rest grouped by length.
 // strict: a single-exponent call fails on an unsupported exponent; a batch marks it and goes on
 // (the reference's batch returns such exponents with seconds < 0, cuda/ll_ntt.cu:259-267).
@@ -346,7 +448,10 @@ int make_batch(const uint64_t* ps, size_t count, uint64_t max_iters, int engine,
             }
             it.n = n;
         }
-        groups[it.n].push_back(it);
+        if (it.n > (1u << kSmallLogMax))
+            b->large.push_back(it);
+        else
+            groups[it.n].push_back(it);
     }
     for (auto& kv : groups) {
         Group g;
@@ -402,9 +507,15 @@ int collect_batch(llg_batch* b) {
         int rc = collect_group(b, g, retry);
         if (rc) return rc;
     }
+    std::vector<Item> large = b->large;
     for (int round = 0; !retry.empty() && round < 16; ++round) {
         std::map<uint32_t, std::vector<Item>> byn;
-        for (Item& it : retry) byn[it.n].push_back(it);
+        for (Item& it : retry) {
+            if (it.n > (1u << kSmallLogMax))
+                large.push_back(it);
+            else
+                byn[it.n].push_back(it);
+        }
         retry.clear();
         for (auto& kv : byn) {
             Group g;
@@ -419,6 +530,22 @@ int collect_batch(llg_batch* b) {
             release_group(g);
             if (rc) return rc;
         }
+    }
+    if (!large.empty()) {
+        cudaStream_t st = b->groups.empty() ? nullptr : b->groups[0].st;
+        cudaStream_t own = nullptr;
+        if (!st) {
+            CK(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
+            st = own;
+        }
+        for (const Item& it : large) {
+            const int rc = run_large(it, b->out[it.idx], b->keep_words ? &b->words[it.idx] : nullptr, st);
+            if (rc) {
+                if (own) cudaStreamDestroy(own);
+                return rc;
+            }
+        }
+        if (own) cudaStreamDestroy(own);
     }
     b->collected = true;
     return LLG_OK;
@@ -498,7 +625,7 @@ uint32_t llg_ntt_length(uint64_t p) {
 }
 
 uint64_t llg_max_exponent(int engine) {
-    if (engine == LLG_ENGINE_FP64) return (uint64_t)std::floor(g_max_bpw * (double)(1u << kSmallLogMax));
+    if (engine == LLG_ENGINE_FP64) return (uint64_t)std::floor(g_max_bpw * (double)(1u << kLargeLogMax));
     return 0;
 }
 
@@ -585,5 +712,87 @@ int llg_batch_device_ms(llg_batch* b, float* ms) {
 }
 
 void llg_batch_destroy(llg_batch* b) { destroy_batch(b); }
+
+}  // extern "C"
+
+struct llg_test {
+    llg::LargeTest T;
+    int dev = -1;
+};
+
+extern "C" {
+
+int llg_test_create(uint64_t p, uint32_t n, llg_test** out) {
+    if (!out) return fail(LLG_E_ARG, "null pointer");
+    *out = nullptr;
+    int dev;
+    int rc = device_ready(&dev);
+    if (rc) return rc;
+    if (p < 3 || p % 2 == 0) return fail(LLG_E_ARG, "p must be odd and >= 3");
+    if (n == 0) n = fp64_length(p, g_max_bpw);
+    const int l = ilog2_exact(n);
+    if (l <= kSmallLogMax || !large_length_supported(l) || !fp64_length_usable(p, n))
+        return fail(LLG_E_UNSUPPORTED, "length %u not usable by the two-pass engine for p=%llu", n,
+                    (unsigned long long)p);
+    llg_test* t = new llg_test();
+    t->dev = dev;
+    cudaError_t e = t->T.init(p, l);
+    if (e != cudaSuccess) {
+        delete t;
+        return fail(e == cudaErrorMemoryAllocation ? LLG_E_NOMEM : LLG_E_CUDA, "CUDA: %s", cudaGetErrorString(e));
+    }
+    *out = t;
+    return LLG_OK;
+}
+
+int llg_test_start(llg_test* t, void* stream) {
+    if (!t) return fail(LLG_E_ARG, "null test");
+    cudaStream_t st = stream ? (cudaStream_t)stream : default_stream_for_thread();
+    CK(t->T.start(seed_digits(1ull << t->T.logN), st));
+    return LLG_OK;
+}
+
+int llg_test_iterate(llg_test* t, uint64_t iters, void* stream) {
+    if (!t) return fail(LLG_E_ARG, "null test");
+    cudaStream_t st = stream ? (cudaStream_t)stream : default_stream_for_thread();
+    CK(t->T.step(iters, st));
+    return LLG_OK;
+}
+
+int llg_test_read(llg_test* t, void* stream, llg_result* out, uint64_t* words, size_t nwords) {
+    if (!t || !out) return fail(LLG_E_ARG, "null pointer");
+    const uint64_t p = t->T.p;
+    const size_t nw = (size_t)((p + 63) / 64);
+    if (words && nwords < nw) return fail(LLG_E_ARG, "words buffer too small");
+    cudaStream_t st = stream ? (cudaStream_t)stream : default_stream_for_thread();
+    std::vector<int> digits;
+    CK(t->T.finish(st, digits));
+    LargeCtl h;
+    CK(t->T.read_ctl(h, st));
+    std::memset(out, 0, sizeof *out);
+    out->p = p;
+    out->iters = t->T.done;
+    out->n = 1u << t->T.logN;
+    out->max_err = bits_to_double(h.err_max);
+    if (h.timeout) return fail(LLG_E_TIMEOUT, "carry wait timed out");
+    std::vector<int64_t> d64(digits.begin(), digits.end());
+    int32_t z = 0;
+    int rc = llg_residue_from_digits(p, out->n, d64.data(), words, words ? nwords : 0, &out->res64, &z);
+    if (rc) return rc;
+    out->is_zero = z;
+    out->status = out->max_err > kAbortErrLarge ? LLG_E_ROUNDOFF : LLG_OK;
+    return LLG_OK;
+}
+
+int llg_test_errlog(llg_test* t, float* log, size_t cap, size_t* len) {
+    if (!t || !log) return fail(LLG_E_ARG, "null pointer");
+    const size_t have = (size_t)std::min<uint64_t>(t->T.done, (uint64_t)t->T.errlog_len);
+    const size_t n = std::min(cap, have);
+    CK(cudaMemcpy(log, t->T.errlog, n * sizeof(float), cudaMemcpyDeviceToHost));
+    if (len) *len = n;
+    return LLG_OK;
+}
+
+void llg_test_destroy(llg_test* t) { delete t; }
 
 }  // extern "C"

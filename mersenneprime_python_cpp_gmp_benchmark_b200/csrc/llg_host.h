@@ -1,0 +1,47 @@
+// Host-side objects of the two-pass engine (internal; not part of the public ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "llg_internal.h"
+
+namespace llg {
+
+constexpr int kGraphChunk = 64;  // squarings per captured CUDA graph
+
+bool large_length_supported(int log_n);
+cudaError_t configure_large(int log_c, int log_r);
+std::vector<int> seed_digits(uint64_t n);
+
+struct LargeTest {
+    uint64_t p = 0, M = 0;
+    int logN = 0, logC = 0, logR = 0, C = 0, R = 0, nblocks = 0;
+    double2* V = nullptr;
+    long long* carry = nullptr;
+    int* carry2 = nullptr;
+    LargeCtl* ctl = nullptr;
+    int* digits = nullptr;
+    float* errlog = nullptr;
+    int errlog_len = 0;
+    double2 *qtwC = nullptr, *qtwR = nullptr, *tw1 = nullptr, *tw2 = nullptr;
+    int* pos_of_c = nullptr;
+    double *wA = nullptr, *iwA = nullptr, *wB = nullptr, *iwB = nullptr;
+    int *sA = nullptr, *sB = nullptr;
+    LargeArgs args{};
+    cudaGraphExec_t exec = nullptr;
+    uint64_t done = 0;  // squarings enqueued since start()
+
+    ~LargeTest();
+    cudaError_t init(uint64_t p, int log_n);
+    cudaError_t start(const std::vector<int>& digits, cudaStream_t st);  // INIT + first squaring
+    cudaError_t step(uint64_t k, cudaStream_t st);                        // k more squarings
+    cudaError_t step_plain(uint64_t k, bool dump_last, cudaStream_t st);
+    cudaError_t finish(cudaStream_t st, std::vector<int>& out);           // FINAL: digits to host
+    cudaError_t read_ctl(LargeCtl& h, cudaStream_t st);
+    cudaError_t clear_err_since(cudaStream_t st);
+};
+
+}  // namespace llg

@@ -33,4 +33,49 @@ cudaError_t launch_small_fp64(int log_n, const SmallJob* jobs, int njobs, const 
 // p < 64: exact 128-bit word arithmetic, one thread per exponent.
 cudaError_t launch_word(const SmallJob* jobs, int njobs, uint64_t* res, cudaStream_t st);
 
+// ---- two-pass engine (N = 2^16 .. 2^23): state resident in HBM ------------------------------
+
+constexpr int kRowG = 8;              // rows per row-pass block
+constexpr int kLargeMaxBlocks = 1024; // row blocks (R / kRowG) supported by the control block
+
+struct LargeCtl {
+    unsigned int epoch;              // squarings whose column pass has finished; +1 per column pass
+    unsigned int ticket[2];          // row-pass block tickets, alternating by epoch parity
+    unsigned int timeout;            // set when a bounded wait gave up (the result is then invalid)
+    unsigned long long err_max;      // bits of the max round-off over the run (double, >= 0)
+    unsigned long long err_since;    // same, since the host last cleared it
+    unsigned int flags[kLargeMaxBlocks];  // flags[k] = epoch + 1 once block k published its carries
+};
+
+enum { LARGE_INIT = 0, LARGE_ITER = 1, LARGE_FINAL = 2 };
+
+struct LargeArgs {
+    double2* V;               // state: element (row a, column slot pos) at pos * R + a
+    const double2* qtwC;      // quarter table of the C-point row FFT
+    const double2* qtwR;      // quarter table of the R-point column FFT
+    const double2* tw1;       // e^{-2 pi i x / M}, x < 2^tw_shift
+    const double2* tw2;       // e^{-2 pi i y 2^tw_shift / M}
+    const int* pos_of_c;      // column slot of row-FFT frequency c
+    const double* wA;         // [2R] 2^(sA/N) of digit 2a+e
+    const double* iwA;        // [2R] 2^(-sA/N)
+    const int* sA;            // [2R] (-(2a+e) p) mod N
+    const double* wB;         // [C] 2^(sB/N)
+    const double* iwB;        // [C] 2^(-sB/N) / (4M)
+    const int* sB;            // [C] (-2Rb p) mod N
+    long long* carry;         // [nblocks][C] hop-1 carry-outs of each block's last row
+    int* carry2;              // [nblocks][C] hop-2 carry-outs of each block's last row
+    LargeCtl* ctl;
+    int* digits;              // N int32, natural order (INIT input; dump / FINAL output)
+    float* errlog;            // per-epoch max round-off ring (may be null)
+    int errlog_len;
+    int dump;                 // ITER: also write the digits
+    int tw_shift;
+    int C, R, nblocks;
+    int q, rem;               // p / N, p % N
+    int logN;
+};
+
+cudaError_t launch_large_row(int log_c, int mode, const LargeArgs& a, cudaStream_t st);
+cudaError_t launch_large_col(int log_r, const LargeArgs& a, cudaStream_t st);
+
 }  // namespace llg

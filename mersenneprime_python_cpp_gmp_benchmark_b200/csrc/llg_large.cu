@@ -1,0 +1,477 @@
+// Two-pass FP64 IBDWT squaring for N = 2^16 .. 2^23 with the residue resident in HBM.
+//
+// The M = N/2 packed complex values u_m (m = a + R*b: row a < R, column b < C, M = R*C) are
+// transformed by the four-step method. One squaring is two kernels, i.e. two read+write sweeps of
+// the 16*M-byte state -- the fewest a transform of this size allows when each pass's working set
+// must fit on chip (the reference does one monolithic FFTW transform per direction,
+// lucaslehmer.cpp:283,288, and an O(N) host loop for each of weight, unweight and carry,
+// lucaslehmer.cpp:282,289-310):
+//
+//   row pass (one block = kRowG consecutive rows, all C columns):
+//       conj twiddle w_M^{-ac}, inverse C-point FFT          (end of the previous squaring)
+//       unweight, round, max round-off, carry, "- 2"
+//       weight, forward C-point FFT, twiddle w_M^{ac}        (start of this squaring)
+//   column pass (one block = the column pair c, C-c):
+//       forward R-point FFT, real-FFT split + pointwise square over the pair (k, M-k),
+//       inverse R-point FFT
+//
+// The state is stored column-slot-major (element (a, pos) at pos*R + a), so a row block reads
+// and writes kRowG contiguous complex values (128 bytes) per column slot and a column block reads
+// and writes its columns contiguously.
+//
+// Carry. Digits 2m, 2m+1 of row a carry into row a+1 (m -> m+1 is a -> a+1), so the chain runs
+// down the rows of each column b. Each row's carry-out is computed from that row's rounded values
+// alone (two-digit chain started at zero); the incoming carry is folded into the first digit and
+// the small remainder into the second, which keeps every digit within a few units of balanced and
+// makes carry-outs independent of carry-ins. Inside a block the carries pass through shared
+// memory; between blocks block k publishes its last row's carry-outs and a flag, and block k+1
+// reads them after a bounded wait. Blocks take tickets in launch order, so the block waited on is
+// always resident or finished. The wrap-around carry into row 0 (2^p == 1) comes from row R-1;
+// block 0 recomputes that row itself instead of waiting on the last block.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "llg_device.cuh"
+#include "llg_fft.cuh"
+#include "llg_host.h"
+#include "llg_internal.h"
+
+namespace llg {
+
+namespace {
+
+constexpr unsigned long long kSpinLimit = 1ull << 22;  // x ~64 ns: ~0.3 s, then give up + flag
+
+__device__ __forceinline__ double2 twiddle_M(const LargeArgs& A, uint32_t x, bool inv) {
+    const double2 a = __ldg(A.tw1 + (x & ((1u << A.tw_shift) - 1u)));
+    const double2 b = __ldg(A.tw2 + (x >> A.tw_shift));
+    const double2 w = cmul(a, b);
+    return inv ? conj2(w) : w;
+}
+
+}  // namespace
+
+template <int LOG_C, int MODE>
+__global__ void __launch_bounds__(kRowG * (1 << LOG_C) / 16, 1) large_row(const LargeArgs A) {
+    using GC = SmallG<LOG_C>;
+    constexpr int C = GC::M, TR = GC::T, E = 16, G = kRowG, T = G * TR;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* bufs = reinterpret_cast<double*>(smem_raw);                  // G x (re, im) x PAD
+    double2* qtw = reinterpret_cast<double2*>(bufs + 2 * G * GC::PAD);   // C/4
+    long long* hin = reinterpret_cast<long long*>(qtw + C / 4);  // C: wrap carry into row 0 (hop 2)
+    long long* hc1 = hin + C;                                     // C: row R-2's carry-out (block 0)
+    int* hin2 = reinterpret_cast<int*>(hc1 + C);                  // C: wrap carry into row 0 (hop 3)
+    long long* carr = reinterpret_cast<long long*>(bufs);         // G x C hop-1 carry-outs (reuses bufs)
+    int* carr2 = reinterpret_cast<int*>(carr + G * C);            // G x C hop-2 carry-outs
+    __shared__ unsigned long long s_err;
+    __shared__ int s_blk;
+    __shared__ unsigned s_epoch;
+
+    const int t = threadIdx.x, rg = t / TR, tr = t % TR;
+    double* sre = bufs + rg * 2 * GC::PAD;
+    double* sim = sre + GC::PAD;
+    const int N = 1 << A.logN, R = A.R;
+
+    if (t == 0) {
+        const unsigned ep = *reinterpret_cast<volatile unsigned*>(&A.ctl->epoch);
+        s_epoch = ep;
+        if (MODE == LARGE_INIT) {
+            s_blk = blockIdx.x;
+        } else {
+            const int b = (int)atomicAdd(&A.ctl->ticket[ep & 1], 1u);
+            if (b == A.nblocks - 1) A.ctl->ticket[(ep + 1) & 1] = 0u;
+            s_blk = b;
+        }
+        s_err = 0ull;
+    }
+    for (int k = t; k < C / 4; k += T) qtw[k] = A.qtwC[k];
+    __syncthreads();
+    const int blk = s_blk;
+    const unsigned ep = s_epoch;
+    const int a0 = blk * G;
+    const int a = a0 + rg;
+
+    double2 v[E];
+    int x0s[E], x1s[E];
+    double lerr = 0.0;
+
+    // per-row weight halves (digits 2a and 2a+1)
+    const int sA0 = __ldg(A.sA + 2 * a), sA1 = __ldg(A.sA + 2 * a + 1);
+
+    if constexpr (MODE == LARGE_INIT) {
+#pragma unroll
+        for (int i = 0; i < E; ++i) {
+            const int b = tr + TR * i;
+            const size_t m = (size_t)a + (size_t)R * b;
+            const int2 d = *reinterpret_cast<const int2*>(A.digits + 2 * m);
+            x0s[i] = d.x;
+            x1s[i] = d.y;
+        }
+    } else {
+        // ---- wrap-around carries into row 0 (2^p == 1): block 0 recomputes rows R-2 and R-1
+        //      (every row group runs the same computation so the FFT's barriers stay uniform).
+        //      Row R-1, column b feeds row 0, column b+1; column C-1 wraps to digit 0. ----
+        if (blk == 0) {
+#pragma unroll 1
+            for (int hrow = 0; hrow < 2; ++hrow) {
+                const int ah = R - 2 + hrow;
+#pragma unroll
+                for (int j = 0; j < E; ++j) {
+                    const int pos = tr * E + j;
+                    const double2 w = A.V[(size_t)pos * R + ah];
+                    const int c = freq_of_pos<GC>(pos);
+                    v[j] = cmul(w, twiddle_M(A, (uint32_t)ah * (uint32_t)c, true));
+                }
+                inverse_from<GC, GC::P - 1>(v, sre, sim, qtw, tr);
+                const int h0 = __ldg(A.sA + 2 * ah), h1 = __ldg(A.sA + 2 * ah + 1);
+                const double ih0 = __ldg(A.iwA + 2 * ah), ih1 = __ldg(A.iwA + 2 * ah + 1);
+#pragma unroll
+                for (int i = 0; i < E; ++i) {
+                    const int b = tr + TR * i;
+                    const int sb = __ldg(A.sB + b);
+                    const double iwb = __ldg(A.iwB + b);
+                    const bool o0 = h0 + sb >= N, o1 = h1 + sb >= N;
+                    const int s0 = o0 ? h0 + sb - N : h0 + sb, s1 = o1 ? h1 + sb - N : h1 + sb;
+                    const int b0 = A.q + (s0 < A.rem), b1 = A.q + (s1 < A.rem);
+                    const double va = v[i].x * (ih0 * iwb) * (o0 ? 2.0 : 1.0);
+                    const double vb = v[i].y * (ih1 * iwb) * (o1 ? 2.0 : 1.0);
+                    long long la, lb, c;
+                    const double ra = round_shift(va, la), rb = round_shift(vb, lb);
+                    lerr = fmax(lerr, fmax(fabs(va - ra), fabs(vb - rb)));
+                    long long x0 = balance(la, b0, c);
+                    long long x1 = balance(lb + c, b1, c);
+                    const long long cout = c;
+                    if (hrow == 0) {
+                        if (rg == 0) hc1[b] = cout;
+                    } else {
+                        // second hop of row R-1 with row R-2's carry-out (same column)
+                        x0 = balance(x0 + hc1[b], b0, c);
+                        balance(x1 + c, b1, c);
+                        if (rg == 0) {
+                            hin[(b + 1) & (C - 1)] = cout;
+                            hin2[(b + 1) & (C - 1)] = (int)c;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+
+        // ---- load the block's rows (coalesced: kRowG contiguous values per column slot) ----
+        {
+            double2 tmp[G * C / T];
+#pragma unroll
+            for (int r = 0; r < G * C / T; ++r) {
+                const int qq = t + T * r, pos = qq / G, ra = qq % G;
+                tmp[r] = A.V[(size_t)pos * R + a0 + ra];
+            }
+#pragma unroll
+            for (int r = 0; r < G * C / T; ++r) {
+                const int qq = t + T * r, pos = qq / G, ra = qq % G;
+                const int x = phys(pos);
+                bufs[ra * 2 * GC::PAD + x] = tmp[r].x;
+                bufs[ra * 2 * GC::PAD + GC::PAD + x] = tmp[r].y;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < E; ++j) {
+            const int pos = tr * E + j;
+            const int x = phys(pos);
+            const int c = freq_of_pos<GC>(pos);
+            v[j] = cmul(make_double2(sre[x], sim[x]), twiddle_M(A, (uint32_t)a * (uint32_t)c, true));
+        }
+        inverse_from<GC, GC::P - 1>(v, sre, sim, qtw, tr);
+        __syncthreads();  // the exchange buffers become the carry arrays
+
+        // ---- carry. Hop 1: unweight, round, round-off, two-digit chain per (row, column) from
+        //      zero: its carry-out goes to the next row. Hop 2: the incoming carry is folded into
+        //      the row's two digits; what leaves the second digit (a few units) goes to the next
+        //      row's first digit (hop 3, not renormalized). Carry-outs of hops 1 and 2 do not
+        //      depend on the previous block, so a block publishes both before waiting. ----
+        const double ia0 = __ldg(A.iwA + 2 * a), ia1 = __ldg(A.iwA + 2 * a + 1);
+#pragma unroll
+        for (int i = 0; i < E; ++i) {
+            const int b = tr + TR * i;
+            const int sb = __ldg(A.sB + b);
+            const double iwb = __ldg(A.iwB + b);
+            const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
+            const int s0 = o0 ? sA0 + sb - N : sA0 + sb, s1 = o1 ? sA1 + sb - N : sA1 + sb;
+            const double va = v[i].x * (ia0 * iwb) * (o0 ? 2.0 : 1.0);
+            const double vb = v[i].y * (ia1 * iwb) * (o1 ? 2.0 : 1.0);
+            long long la, lb, c;
+            const double ra = round_shift(va, la), rb = round_shift(vb, lb);
+            lerr = fmax(lerr, fmax(fabs(va - ra), fabs(vb - rb)));
+            const long long x0 = balance(la, A.q + (s0 < A.rem), c);
+            const long long x1 = balance(lb + c, A.q + (s1 < A.rem), c);
+            x0s[i] = (int)x0;
+            x1s[i] = (int)x1;
+            carr[rg * C + b] = c;
+            if (rg == G - 1) A.carry[(size_t)blk * C + b] = c;
+        }
+        atomicMax(&s_err, (unsigned long long)__double_as_longlong(lerr));
+        __syncthreads();
+        // hop 2 for rows fed from inside the block
+        if (rg > 0) {
+#pragma unroll
+            for (int i = 0; i < E; ++i) {
+                const int b = tr + TR * i;
+                const int sb = __ldg(A.sB + b);
+                const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
+                const int s0 = o0 ? sA0 + sb - N : sA0 + sb, s1 = o1 ? sA1 + sb - N : sA1 + sb;
+                long long c;
+                x0s[i] = (int)balance((long long)x0s[i] + carr[(rg - 1) * C + b], A.q + (s0 < A.rem), c);
+                x1s[i] = (int)balance((long long)x1s[i] + c, A.q + (s1 < A.rem), c);
+                carr2[rg * C + b] = (int)c;
+                if (rg == G - 1) A.carry2[(size_t)blk * C + b] = (int)c;
+            }
+        }
+        __threadfence();  // each writer orders its carry-out stores before the flag below
+        __syncthreads();
+        if (t == 0) {
+            __threadfence();
+            *reinterpret_cast<volatile unsigned*>(&A.ctl->flags[blk]) = ep + 1u;
+            if (blk > 0) {
+                // wait (bounded) for block blk-1's carry-outs
+                volatile unsigned* f = &A.ctl->flags[blk - 1];
+                unsigned long long spins = 0;
+                while (*f < ep + 1u) {
+                    if (++spins > kSpinLimit) {
+                        atomicExch(&A.ctl->timeout, 1u);
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+                __threadfence();
+            }
+        }
+        __syncthreads();
+        // hop 2 for the block's first row: previous block's last row, or the wrap
+        if (rg == 0) {
+#pragma unroll
+            for (int i = 0; i < E; ++i) {
+                const int b = tr + TR * i;
+                long long cin = (blk > 0) ? __ldcg(A.carry + (size_t)(blk - 1) * C + b) : hin[b];
+                if (a == 0 && b == 0) cin -= 2;  // the "- 2" of s^2 - 2 (digit 0)
+                const int sb = __ldg(A.sB + b);
+                const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
+                const int s0 = o0 ? sA0 + sb - N : sA0 + sb, s1 = o1 ? sA1 + sb - N : sA1 + sb;
+                long long c;
+                x0s[i] = (int)balance((long long)x0s[i] + cin, A.q + (s0 < A.rem), c);
+                x1s[i] = (int)balance((long long)x1s[i] + c, A.q + (s1 < A.rem), c);
+                carr2[b] = (int)c;
+            }
+        }
+        __syncthreads();
+        // hop 3: the small second-digit carry of the previous row into this row's first digit
+#pragma unroll
+        for (int i = 0; i < E; ++i) {
+            const int b = tr + TR * i;
+            int c2;
+            if (rg > 0)
+                c2 = carr2[(rg - 1) * C + b];
+            else if (blk > 0)
+                c2 = __ldcg(A.carry2 + (size_t)(blk - 1) * C + b);
+            else
+                c2 = hin2[b];
+            x0s[i] += c2;
+        }
+        if (MODE == LARGE_FINAL || A.dump) {
+#pragma unroll
+            for (int i = 0; i < E; ++i) {
+                const int b = tr + TR * i;
+                const size_t m = (size_t)a + (size_t)R * b;
+                *reinterpret_cast<int2*>(A.digits + 2 * m) = make_int2(x0s[i], x1s[i]);
+            }
+        }
+        if (t == 0) {
+            const unsigned long long eb = s_err;
+            atomicMax(&A.ctl->err_max, eb);
+            atomicMax(&A.ctl->err_since, eb);
+            if (A.errlog) atomicMax(reinterpret_cast<unsigned int*>(A.errlog + (ep % (unsigned)A.errlog_len)),
+                                    __float_as_uint((float)__longlong_as_double((long long)eb)));
+        }
+        if constexpr (MODE == LARGE_FINAL) return;
+        __syncthreads();  // carry array reads done before the exchange buffers are reused
+    }
+
+    // ---- weight, forward row FFT, twiddle, store ----
+    const double wa0 = __ldg(A.wA + 2 * a), wa1 = __ldg(A.wA + 2 * a + 1);
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+        const int b = tr + TR * i;
+        const int sb = __ldg(A.sB + b);
+        const double wb = __ldg(A.wB + b);
+        const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
+        v[i].x = i2d_shift(x0s[i]) * (wa0 * wb) * (o0 ? 0.5 : 1.0);
+        v[i].y = i2d_shift(x1s[i]) * (wa1 * wb) * (o1 ? 0.5 : 1.0);
+    }
+    forward_from<GC, 0>(v, sre, sim, qtw, tr);
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+        const int pos = tr * E + j;
+        const int c = freq_of_pos<GC>(pos);
+        const double2 w = cmul(v[j], twiddle_M(A, (uint32_t)a * (uint32_t)c, false));
+        const int x = phys(pos);
+        sre[x] = w.x;
+        sim[x] = w.y;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < G * C / T; ++r) {
+        const int qq = t + T * r, pos = qq / G, ra = qq % G;
+        const int x = phys(pos);
+        A.V[(size_t)pos * R + a0 + ra] =
+            make_double2(bufs[ra * 2 * GC::PAD + x], bufs[ra * 2 * GC::PAD + GC::PAD + x]);
+    }
+}
+
+template <int LOG_R>
+__global__ void __launch_bounds__(2 * (1 << LOG_R) / 16, 1) large_col(const LargeArgs A) {
+    using GR = SmallG<LOG_R>;
+    constexpr int R = GR::M, TC = GR::T, E = 16;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* bufs = reinterpret_cast<double*>(smem_raw);                 // 2 x (re, im) x PAD
+    double2* qtw = reinterpret_cast<double2*>(bufs + 4 * GR::PAD);       // R/4
+    const int t = threadIdx.x, half = t / TC, tc = t % TC;
+    const int C = A.C;
+    const int cb = blockIdx.x;  // 0 .. C/2
+    const int c1 = cb, c2 = (C - cb) & (C - 1);
+    const bool self = (c1 == c2);
+    const bool active = !(self && half == 1);
+    const int c = half ? c2 : c1;
+    double* sre = bufs + half * 2 * GR::PAD;
+    double* sim = sre + GR::PAD;
+    const double* pre = self ? sre : bufs + (1 - half) * 2 * GR::PAD;  // partner column
+    const double* pim = pre + GR::PAD;
+    for (int k = t; k < R / 4; k += 2 * TC) qtw[k] = A.qtwR[k];
+    double2* col = A.V + (size_t)__ldg(A.pos_of_c + c) * R;
+    double2 v[E];
+#pragma unroll
+    for (int i = 0; i < E; ++i) v[i] = active ? col[tc + TC * i] : make_double2(0.0, 0.0);
+    __syncthreads();
+    forward_from<GR, 0>(v, sre, sim, qtw, tc);
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+        const int x = phys(tc * E + j);
+        sre[x] = v[j].x;
+        sim[x] = v[j].y;
+    }
+    __syncthreads();
+    const double2 wc = __ldg(A.tw1 + c);  // w_M^c
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+        const int d = freq_of_pos<GR>(tc * E + j);
+        const int dp = (c == 0) ? ((R - d) & (R - 1)) : (R - 1 - d);
+        const int xp = phys(pos_of_freq<GR>(dp));
+        const double2 Av = v[j], Bc = make_double2(pre[xp], -pim[xp]);  // conj(U_{M-k})
+        const double2 s = cadd(Av, Bc), dd = csub(Av, Bc);
+        const double2 a3 = make_double2(3.0 * Av.x - Bc.x, 3.0 * Av.y - Bc.y);
+        const double2 d2 = make_double2((dd.x - dd.y) * (dd.x + dd.y), 2.0 * dd.x * dd.y);
+        const double2 w = cmul(wc, twiddle<LOG_R>(qtw, (uint32_t)d, false));  // w_M^{c + C d}
+        v[j] = csub(cmul(a3, s), cmul(w, d2));
+    }
+    inverse_from<GR, GR::P - 1>(v, sre, sim, qtw, tc);
+    if (active) {
+#pragma unroll
+        for (int i = 0; i < E; ++i) col[tc + TC * i] = v[i];
+    }
+    if (cb == 0 && t == 0) atomicAdd(&A.ctl->epoch, 1u);
+}
+
+template <int LOG_C>
+static size_t row_smem() {
+    using GC = SmallGeom<LOG_C>;
+    return sizeof(double) * 2 * kRowG * GC::PAD + sizeof(double2) * (GC::M / 4) + 2 * sizeof(long long) * GC::M +
+           sizeof(int) * GC::M;
+}
+
+template <int LOG_R>
+static size_t col_smem() {
+    using GR = SmallGeom<LOG_R>;
+    return sizeof(double) * 4 * GR::PAD + sizeof(double2) * (GR::M / 4);
+}
+
+template <int LOG_C, int MODE>
+static cudaError_t row_attr() {
+    return cudaFuncSetAttribute(large_row<LOG_C, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)row_smem<LOG_C>());
+}
+
+template <int LOG_R>
+static cudaError_t col_attr() {
+    return cudaFuncSetAttribute(large_col<LOG_R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)col_smem<LOG_R>());
+}
+
+template <int LOG_C, int MODE>
+static cudaError_t row_t(const LargeArgs& a, cudaStream_t st) {
+    large_row<LOG_C, MODE><<<a.nblocks, kRowG * (1 << LOG_C) / 16, row_smem<LOG_C>(), st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int LOG_R>
+static cudaError_t col_t(const LargeArgs& a, cudaStream_t st) {
+    large_col<LOG_R><<<a.C / 2 + 1, 2 * (1 << LOG_R) / 16, col_smem<LOG_R>(), st>>>(a);
+    return cudaGetLastError();
+}
+
+// Opts the kernels of one geometry into their dynamic shared memory (once per device, before
+// any launch or graph capture).
+cudaError_t configure_large(int log_c, int log_r) {
+    cudaError_t e = cudaSuccess;
+    switch (log_c) {
+        case 6: if (!(e = row_attr<6, LARGE_INIT>()) && !(e = row_attr<6, LARGE_ITER>())) e = row_attr<6, LARGE_FINAL>(); break;
+        case 7: if (!(e = row_attr<7, LARGE_INIT>()) && !(e = row_attr<7, LARGE_ITER>())) e = row_attr<7, LARGE_FINAL>(); break;
+        case 8: if (!(e = row_attr<8, LARGE_INIT>()) && !(e = row_attr<8, LARGE_ITER>())) e = row_attr<8, LARGE_FINAL>(); break;
+        case 9: if (!(e = row_attr<9, LARGE_INIT>()) && !(e = row_attr<9, LARGE_ITER>())) e = row_attr<9, LARGE_FINAL>(); break;
+        case 10: if (!(e = row_attr<10, LARGE_INIT>()) && !(e = row_attr<10, LARGE_ITER>())) e = row_attr<10, LARGE_FINAL>(); break;
+        default: return cudaErrorInvalidValue;
+    }
+    if (e) return e;
+    switch (log_r) {
+        case 7: return col_attr<7>();
+        case 8: return col_attr<8>();
+        case 9: return col_attr<9>();
+        case 10: return col_attr<10>();
+        case 11: return col_attr<11>();
+        case 12: return col_attr<12>();
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int MODE>
+static cudaError_t row_mode(int log_c, const LargeArgs& a, cudaStream_t st) {
+    switch (log_c) {
+        case 6: return row_t<6, MODE>(a, st);
+        case 7: return row_t<7, MODE>(a, st);
+        case 8: return row_t<8, MODE>(a, st);
+        case 9: return row_t<9, MODE>(a, st);
+        case 10: return row_t<10, MODE>(a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_large_row(int log_c, int mode, const LargeArgs& a, cudaStream_t st) {
+    switch (mode) {
+        case LARGE_INIT: return row_mode<LARGE_INIT>(log_c, a, st);
+        case LARGE_ITER: return row_mode<LARGE_ITER>(log_c, a, st);
+        case LARGE_FINAL: return row_mode<LARGE_FINAL>(log_c, a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_large_col(int log_r, const LargeArgs& a, cudaStream_t st) {
+    switch (log_r) {
+        case 7: return col_t<7>(a, st);
+        case 8: return col_t<8>(a, st);
+        case 9: return col_t<9>(a, st);
+        case 10: return col_t<10>(a, st);
+        case 11: return col_t<11>(a, st);
+        case 12: return col_t<12>(a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace llg

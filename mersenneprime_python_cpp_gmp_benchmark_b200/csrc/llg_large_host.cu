@@ -1,0 +1,232 @@
+// Host side of the two-pass engine: per-test device state, tables, the launch sequence of a
+// squaring (row pass, column pass), CUDA-graph capture of chunks of squarings, read-back.
+//
+// Launch sequence for k squarings from given digits:  row(INIT), col, [row(ITER), col] x (k-1),
+// row(FINAL). Every row pass after the first finishes the previous squaring (inverse row FFT,
+// carry) and starts the next (forward row FFT); every column pass is one pointwise square.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstring>
+#include <vector>
+
+#include "../../include/llgpu.h"
+#include "llg_host.h"
+#include "llg_internal.h"
+
+namespace llg {
+
+namespace {
+
+int ilog2(uint64_t n) {
+    int l = 0;
+    while ((1ull << l) < n) ++l;
+    return l;
+}
+
+// mixed-radix (16, ..., 16, RLAST) digit reversal of the L-point FFT (host copy of pos_of_freq)
+int host_pos_of_freq(int log_l, int k) {
+    const int L = 1 << log_l, P = (log_l + 3) / 4;
+    const int RLAST = (log_l % 4 == 0) ? 16 : (1 << (log_l % 4));
+    const int klast = k / (L / RLAST);
+    int low = k % (L / RLAST), rest = 0;
+    for (int s = 0; s < P - 1; ++s) {
+        rest = (rest << 4) | (low & 15);
+        low >>= 4;
+    }
+    return rest * RLAST + klast;
+}
+
+std::vector<double2> omega_table(uint64_t period, uint64_t count, uint64_t step) {
+    // e^{-2 pi i x step / period}, x < count, rounded once from long double
+    std::vector<double2> t(count);
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    for (uint64_t x = 0; x < count; ++x) {
+        const uint64_t e = (x * step) % period;
+        const long double ang = two_pi * (long double)e / (long double)period;
+        t[x] = make_double2((double)cosl(ang), -(double)sinl(ang));
+    }
+    return t;
+}
+
+template <class T>
+cudaError_t upload(T** d, const std::vector<T>& h) {
+    cudaError_t e = cudaMalloc(d, h.size() * sizeof(T));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+}  // namespace
+
+bool large_length_supported(int log_n) { return log_n >= 14 && log_n <= 23; }
+
+LargeTest::~LargeTest() {
+    if (exec) cudaGraphExecDestroy(exec);
+    void* ptrs[] = {V, carry, carry2, ctl, digits, errlog, qtwC, qtwR, tw1, tw2, pos_of_c, wA, iwA, sA, wB, iwB, sB};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+}
+
+cudaError_t LargeTest::init(uint64_t p_, int log_n) {
+    p = p_;
+    logN = log_n;
+    const uint64_t N = 1ull << logN;
+    M = N / 2;
+    logC = (logN <= 15) ? logN - 8 : (logN <= 17) ? 8 : (logN <= 19) ? 9 : 10;
+    logR = logN - 1 - logC;
+    C = 1 << logC;
+    R = 1 << logR;
+    nblocks = R / kRowG;
+    const int s = std::max(logC, (int)((logN - 1 + 1) / 2));
+    cudaError_t e;
+    if ((e = configure_large(logC, logR))) return e;
+    // tables
+    if ((e = upload(&qtwC, omega_table(C, C / 4, 1)))) return e;
+    if ((e = upload(&qtwR, omega_table(R, R / 4, 1)))) return e;
+    if ((e = upload(&tw1, omega_table(M, 1ull << s, 1)))) return e;
+    if ((e = upload(&tw2, omega_table(M, M >> s, 1ull << s)))) return e;
+    std::vector<int> pc(C);
+    for (int c = 0; c < C; ++c) pc[c] = host_pos_of_freq(logC, c);
+    if ((e = upload(&pos_of_c, pc))) return e;
+    std::vector<double> hwA(2 * R), hiwA(2 * R), hwB(C), hiwB(C);
+    std::vector<int> hsA(2 * R), hsB(C);
+    const long double Nl = (long double)N;
+    for (int j = 0; j < 2 * R; ++j) {
+        const uint64_t sj = (N - (uint64_t)(((unsigned __int128)j * p) % N)) % N;
+        hsA[j] = (int)sj;
+        hwA[j] = (double)exp2l((long double)sj / Nl);
+        hiwA[j] = (double)exp2l(-(long double)sj / Nl);
+    }
+    for (int b = 0; b < C; ++b) {
+        const uint64_t sj = (N - (uint64_t)(((unsigned __int128)2 * R * b * p) % N)) % N;
+        hsB[b] = (int)sj;
+        hwB[b] = (double)exp2l((long double)sj / Nl);
+        hiwB[b] = (double)(exp2l(-(long double)sj / Nl) / (4.0L * (long double)M));
+    }
+    if ((e = upload(&wA, hwA))) return e;
+    if ((e = upload(&iwA, hiwA))) return e;
+    if ((e = upload(&sA, hsA))) return e;
+    if ((e = upload(&wB, hwB))) return e;
+    if ((e = upload(&iwB, hiwB))) return e;
+    if ((e = upload(&sB, hsB))) return e;
+    // state
+    if ((e = cudaMalloc(&V, M * sizeof(double2)))) return e;
+    if ((e = cudaMalloc(&carry, (size_t)nblocks * C * sizeof(long long)))) return e;
+    if ((e = cudaMalloc(&carry2, (size_t)nblocks * C * sizeof(int)))) return e;
+    if ((e = cudaMalloc(&ctl, sizeof(LargeCtl)))) return e;
+    if ((e = cudaMemset(ctl, 0, sizeof(LargeCtl)))) return e;
+    if ((e = cudaMalloc(&digits, N * sizeof(int)))) return e;
+    errlog_len = 1 << 16;
+    if ((e = cudaMalloc(&errlog, errlog_len * sizeof(float)))) return e;
+    if ((e = cudaMemset(errlog, 0, errlog_len * sizeof(float)))) return e;
+
+    LargeArgs& A = args;
+    std::memset(&A, 0, sizeof A);
+    A.V = V;
+    A.qtwC = qtwC;
+    A.qtwR = qtwR;
+    A.tw1 = tw1;
+    A.tw2 = tw2;
+    A.pos_of_c = pos_of_c;
+    A.wA = wA;
+    A.iwA = iwA;
+    A.sA = sA;
+    A.wB = wB;
+    A.iwB = iwB;
+    A.sB = sB;
+    A.carry = carry;
+    A.carry2 = carry2;
+    A.ctl = ctl;
+    A.digits = digits;
+    A.errlog = errlog;
+    A.errlog_len = errlog_len;
+    A.dump = 0;
+    A.tw_shift = s;
+    A.C = C;
+    A.R = R;
+    A.nblocks = nblocks;
+    A.q = (int)(p >> logN);
+    A.rem = (int)(p & (N - 1));
+    A.logN = logN;
+    return cudaSuccess;
+}
+
+cudaError_t LargeTest::start(const std::vector<int>& d, cudaStream_t st) {
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(digits, d.data(), d.size() * sizeof(int), cudaMemcpyHostToDevice, st))) return e;
+    if ((e = cudaMemsetAsync(ctl, 0, sizeof(LargeCtl), st))) return e;
+    if ((e = cudaMemsetAsync(errlog, 0, errlog_len * sizeof(float), st))) return e;
+    if ((e = launch_large_row(logC, LARGE_INIT, args, st))) return e;
+    if ((e = launch_large_col(logR, args, st))) return e;
+    done = 1;
+    return cudaSuccess;
+}
+
+cudaError_t LargeTest::step_plain(uint64_t k, bool dump_last, cudaStream_t st) {
+    cudaError_t e;
+    for (uint64_t i = 0; i < k; ++i) {
+        LargeArgs a = args;
+        a.dump = (dump_last && i + 1 == k) ? 1 : 0;
+        if ((e = launch_large_row(logC, LARGE_ITER, a, st))) return e;
+        if ((e = launch_large_col(logR, a, st))) return e;
+    }
+    done += k;
+    return cudaSuccess;
+}
+
+// k squarings as replays of a captured graph of kGraphChunk (row, col) pairs plus a remainder.
+cudaError_t LargeTest::step(uint64_t k, cudaStream_t st) {
+    cudaError_t e;
+    if (!exec && k >= (uint64_t)kGraphChunk) {
+        cudaStream_t cap;
+        if ((e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking))) return e;
+        if ((e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal))) return e;
+        for (int i = 0; i < kGraphChunk; ++i) {
+            launch_large_row(logC, LARGE_ITER, args, cap);
+            launch_large_col(logR, args, cap);
+        }
+        cudaGraph_t g;
+        e = cudaStreamEndCapture(cap, &g);
+        cudaStreamDestroy(cap);
+        if (e) return e;
+        e = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e) return e;
+    }
+    uint64_t left = k;
+    while (exec && left >= (uint64_t)kGraphChunk) {
+        if ((e = cudaGraphLaunch(exec, st))) return e;
+        left -= kGraphChunk;
+        done += kGraphChunk;
+    }
+    return step_plain(left, false, st);
+}
+
+cudaError_t LargeTest::finish(cudaStream_t st, std::vector<int>& out) {
+    cudaError_t e;
+    if ((e = launch_large_row(logC, LARGE_FINAL, args, st))) return e;
+    out.resize(2 * M);
+    if ((e = cudaMemcpyAsync(out.data(), digits, 2 * M * sizeof(int), cudaMemcpyDeviceToHost, st))) return e;
+    return cudaStreamSynchronize(st);
+}
+
+cudaError_t LargeTest::read_ctl(LargeCtl& h, cudaStream_t st) {
+    cudaError_t e = cudaMemcpyAsync(&h, ctl, offsetof(LargeCtl, flags), cudaMemcpyDeviceToHost, st);
+    if (e) return e;
+    return cudaStreamSynchronize(st);
+}
+
+cudaError_t LargeTest::clear_err_since(cudaStream_t st) {
+    return cudaMemsetAsync(&ctl->err_since, 0, sizeof(unsigned long long), st);
+}
+
+// Balanced digits of s_0 = 4 (digit 0 holds 4; every digit has >= 3 bits here).
+std::vector<int> seed_digits(uint64_t n) {
+    std::vector<int> d(n, 0);
+    d[0] = 4;
+    return d;
+}
+
+}  // namespace llg

@@ -68,6 +68,13 @@ def lib() -> ctypes.CDLL:
         L.llg_measure_peak.argtypes = [ctypes.c_int, P(dbl)]
         L.llg_batch_device_ms.argtypes = [ctypes.c_void_p, P(ctypes.c_float)]
         L.llg_batch_destroy.argtypes = [ctypes.c_void_p]
+        L.llg_test_create.argtypes = [u64, u32, P(ctypes.c_void_p)]
+        L.llg_test_start.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.llg_test_iterate.argtypes = [ctypes.c_void_p, u64, ctypes.c_void_p]
+        L.llg_test_read.argtypes = [ctypes.c_void_p, ctypes.c_void_p, P(LlgResult), P(u64), sz]
+        L.llg_test_errlog.argtypes = [ctypes.c_void_p, P(ctypes.c_float), sz, P(sz)]
+        L.llg_test_destroy.argtypes = [ctypes.c_void_p]
+        L.llg_test_destroy.restype = None
         L.llg_batch_destroy.restype = None
         _lib = L
     return _lib
@@ -181,6 +188,49 @@ class Batch:
     def close(self):
         if self.h:
             lib().llg_batch_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Test:
+    """One exponent on the two-pass engine (llg_test_*): start, iterate on a stream, read."""
+
+    def __init__(self, p, n=0):
+        self.p = p
+        self.h = ctypes.c_void_p()
+        _check(lib().llg_test_create(p, n, ctypes.byref(self.h)))
+
+    def start(self, stream=0):
+        _check(lib().llg_test_start(self.h, ctypes.c_void_p(stream or None)))
+
+    def iterate(self, iters, stream=0):
+        _check(lib().llg_test_iterate(self.h, iters, ctypes.c_void_p(stream or None)))
+
+    def read(self, stream=0, want_words=False):
+        r = LlgResult()
+        nw = nwords(self.p)
+        words = (ctypes.c_uint64 * nw)() if want_words else None
+        _check(lib().llg_test_read(self.h, ctypes.c_void_p(stream or None), ctypes.byref(r), words,
+                                   nw if want_words else 0))
+        d = r.as_dict()
+        if want_words:
+            d["words"] = list(words)
+        return d
+
+    def errlog(self, n):
+        buf = (ctypes.c_float * n)()
+        ln = ctypes.c_size_t()
+        _check(lib().llg_test_errlog(self.h, buf, n, ctypes.byref(ln)))
+        return list(buf[:ln.value])
+
+    def close(self):
+        if self.h:
+            lib().llg_test_destroy(self.h)
             self.h = ctypes.c_void_p()
 
     def __del__(self):

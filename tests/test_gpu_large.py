@@ -1,0 +1,93 @@
+"""Parity of the two-pass engine (lengths 2^14 .. 2^23, state in HBM) with the oracle and with the
+reference's own golden residues, through the C-ABI.
+
+Interim residues are compared in full (every limb) against the oracle's GMP restatement where the
+oracle finishes in seconds, and as res64 against the reference's gmp_res64_after values
+(tests/golden/appendix.json, trace_1257787.json) at the benchmark sizes."""
+import pytest
+
+from conftest import load_json
+
+pytestmark = pytest.mark.gpu
+
+
+def _after():
+    return {(d["p"], d["k"]): int(d["res64"], 16) for d in load_json("appendix.json")["after"]}
+
+
+@pytest.mark.parametrize("logn", range(14, 24))
+def test_every_large_length_full_residue(gpu, oracle, logn):
+    """Every supported two-pass length, a p at ~16.5 bits/digit, past the first wrap-around."""
+    n = 1 << logn
+    p = int(16.5 * n) | 1
+    while any(p % d == 0 for d in (3, 5, 7, 11, 13)):
+        p += 2
+    k = p.bit_length() + 4  # s_k exceeds 2^p after ~log2(p) squarings: the reduction is exercised
+    r = gpu.run(p, iters=k, n=n, want_words=True)
+    assert r["status"] == 0 and r["n"] == n and r["iters"] == k
+    assert r["words"] == oracle.ll_gmp(p, k)[2]
+    assert r["max_err"] < 0.1
+
+
+@pytest.mark.parametrize("p,k", [(1257787, 240), (1257787, 1000), (1257787, 10000)])
+def test_config_p1257787_at_65536(gpu, p, k):
+    """p = 1,257,787 at N = 65536 (19.19 bits/digit), res64 after k vs the reference GMP engine."""
+    r = gpu.run(p, iters=k, n=65536)
+    assert r["status"] == 0 and r["n"] == 65536
+    assert r["res64"] == _after()[(p, k)]
+
+
+def test_config_sweep_primes_1000(gpu):
+    """The 8 seeded primes in [20M, 25M]: res64 after 1000 squarings vs the reference GMP engine.
+    Length chosen at 19.5 bits/digit (2^20 where it fits, else 2^21), escalated on round-off."""
+    g = load_json("appendix.json")
+    after = _after()
+    for p in g["sweep_primes"]:
+        n = gpu.fft_length(p, 19.5)
+        r = gpu.run(p, iters=1000, n=n)
+        assert r["status"] == 0, p
+        assert r["res64"] == after[(p, 1000)], p
+        assert r["max_err"] <= 0.4
+
+
+@pytest.mark.parametrize("k", [34, 1000])
+def test_config_largest_p136279841(gpu, k):
+    """p = 136,279,841 at N = 2^23 (16.25 bits/digit): res64 after k squarings vs the reference."""
+    r = gpu.run(136279841, iters=k, n=1 << 23)
+    assert r["status"] == 0 and r["n"] == 1 << 23
+    assert r["res64"] == _after()[(136279841, k)]
+    assert r["max_err"] < 0.4
+
+
+def test_test_object_interim_and_errlog(gpu, oracle):
+    """llg_test_*: start / iterate in pieces / read equals one run; the round-off log is filled."""
+    p, n = 3021377, 1 << 18
+    t = gpu.Test(p, n)
+    t.start()
+    t.iterate(999)
+    t.iterate(1000)
+    r = t.read(want_words=True)
+    assert r["iters"] == 2000
+    one = gpu.run(p, iters=2000, n=n, want_words=True)
+    assert r["words"] == one["words"]
+    log = t.errlog(2001)
+    assert len(log) >= 2000 and max(log[1:2000]) > 0 and max(log) <= r["max_err"] + 1e-7
+    t.close()
+
+
+def test_readme_interim_residue(gpu):
+    """README.md:204-206: res64 of p = 3,021,377 after 20,000 squarings is ce811e3772129824."""
+    r = gpu.run(3021377, iters=20000)
+    assert r["res64"] == 0xCE811E3772129824
+
+
+def test_large_escalation_exact(gpu, oracle):
+    """A length far too short for FP64 (27 bits/digit at 2^16) aborts on round-off and is redone
+    at a longer length; the residue stays exact."""
+    p = 27 * 65536 - 5
+    while any(p % d == 0 for d in (3, 5, 7, 11, 13)):
+        p -= 2
+    k = 40
+    r = gpu.run(p, iters=k, n=65536, want_words=True)
+    assert r["status"] == 0 and r["escalations"] >= 1 and r["n"] > 65536
+    assert r["words"] == oracle.ll_gmp(p, k)[2]
