@@ -130,6 +130,25 @@ void llg_test_destroy(llg_test* t);
 int llg_residue_from_digits(uint64_t p, uint32_t n, const int64_t* digits, uint64_t* words,
                             size_t nwords, uint64_t* res64, int32_t* is_zero);
 
+/* The two-pass engine for transform lengths 16,384 .. 65,536 without allocating device memory.
+ * No counterpart in the reference: it serves callers that cannot call cudaMalloc (a host
+ * framework that owns every device allocation through its own pool, or code that must not risk
+ * the device-wide synchronisation cudaFree can cause while other work is in flight). All state
+ * and tables live in one fixed device array of LLG_NOALLOC_SCRATCH_BYTES inside this library,
+ * which every GPU that loads the library keeps until the process exits.
+ * n must be a power of two in [16384, LLG_NOALLOC_MAX_N] usable for p (else LLG_E_UNSUPPORTED);
+ * iters >= 1 squarings from s_0 = 4. digits_out: caller-owned DEVICE buffer of n int32 that
+ * receives the balanced digits of s_iters in natural order (llg_residue_from_digits gives the
+ * residue). max_err (host, optional): worst round-off. Enqueues on `stream` (NULL: legacy
+ * default stream) and returns when it has finished; LLG_E_ROUNDOFF if the round-off exceeded 0.4.
+ * Every call reuses the same array and leaves its contents behind; the call zeroes what has to
+ * start at zero. Calls whose GPU work overlaps race on the array: serialise them. The first call
+ * on each device looks up the array's device address; make it outside any stream capture. */
+#define LLG_NOALLOC_MAX_N 65536u
+#define LLG_NOALLOC_SCRATCH_BYTES (640u * 1024u)
+int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* digits_out, double* max_err,
+                    void* stream);
+
 /* Roofline denominators measured on the current device: which = 0 FP64 FMA flops/s,
  * which = 1 INT32 multiply-adds/s (dependent chains on every SM). Diagnostic; no reference
  * counterpart. */

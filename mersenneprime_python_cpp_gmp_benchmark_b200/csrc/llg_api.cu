@@ -572,6 +572,10 @@ int run_sync(llg_batch* b) {
 
 }  // namespace
 
+namespace llg {
+int set_error(int code, const char* msg) { return fail(code, "%s", msg); }
+}  // namespace llg
+
 extern "C" {
 
 const char* llg_status_string(int s) {

@@ -13,6 +13,7 @@ namespace llg {
 constexpr int kGraphChunk = 64;  // squarings per captured CUDA graph
 
 bool large_length_supported(int log_n);
+int set_error(int code, const char* msg);  // records this thread's llg_last_error() text
 cudaError_t configure_large(int log_c, int log_r);
 std::vector<int> seed_digits(uint64_t n);
 

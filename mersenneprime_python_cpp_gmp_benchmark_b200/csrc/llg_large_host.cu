@@ -20,12 +20,6 @@ namespace llg {
 
 namespace {
 
-int ilog2(uint64_t n) {
-    int l = 0;
-    while ((1ull << l) < n) ++l;
-    return l;
-}
-
 // mixed-radix (16, ..., 16, RLAST) digit reversal of the L-point FFT (host copy of pos_of_freq)
 int host_pos_of_freq(int log_l, int k) {
     const int L = 1 << log_l, P = (log_l + 3) / 4;

@@ -1,0 +1,237 @@
+// llg_run_noalloc: the two-pass engine for lengths up to 65,536 without any device allocation.
+//
+// Why it exists: some callers cannot call cudaMalloc -- for example code running inside a host
+// framework that owns every device allocation through its own pool, or a caller that must not
+// trigger the implicit device synchronisation cudaFree can cause while other work is in flight.
+// Every other entry point of this library allocates its state (the residue, the carry buffers,
+// the control block, the twiddle and weight tables) per call or per test object. This one keeps
+// all of that in one fixed-size array in device memory, declared below at file scope, which every
+// GPU that loads this library holds until the process exits (kNoAllocScratchBytes bytes).
+//
+// Rules a caller must know:
+//   * N (the transform length) must be a power of two from 16,384 to 65,536 and usable for p
+//     (the same bits-per-digit rule as the allocating two-pass entry points); anything larger is
+//     rejected with LLG_E_UNSUPPORTED because its state would not fit the array.
+//   * All calls share the one array and it keeps the previous call's contents. The call clears
+//     what must start at zero (the control block) and overwrites everything else before reading
+//     it. Two calls whose GPU work overlaps (different streams, or different host threads) race on
+//     the array and produce wrong results: serialise them.
+//   * The first call on each device looks up the array's device address (cudaGetSymbolAddress);
+//     make that first call outside any stream capture.
+//   * The caller passes the output: digits_out, a device buffer of N int32 values, receives the
+//     balanced digits of s_iters in natural order (llg_residue_from_digits turns them into the
+//     residue). The call enqueues on `stream` (NULL: the legacy default stream) and returns after
+//     that stream has finished.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstddef>
+#include <cstring>
+#include <mutex>
+
+#include "../../include/llgpu.h"
+#include "llg_host.h"
+#include "llg_internal.h"
+
+namespace llg {
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = 640u * 1024u;  // covers N = 65,536 (about 584 KiB used)
+constexpr int kNoAllocMaxLog = 16;
+constexpr int kMaxDevices = 64;
+
+// The scratch itself. In host code this name is only a stand-in for the device copy: its device
+// address comes from cudaGetSymbolAddress (per device) and only that address is given to kernels.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mx;
+unsigned char* g_scratch_addr[kMaxDevices] = {};
+
+// Host staging for the tables (no host allocation either): the largest table set is ~24 KiB.
+constexpr size_t kStageBytes = 64u * 1024u;
+alignas(64) unsigned char g_stage[kStageBytes];
+
+struct Layout {
+    size_t V, carry, carry2, ctl, qtwC, qtwR, tw1, tw2, pos_of_c, wA, iwA, sA, wB, iwB, sB, end;
+};
+
+size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+Layout layout(int logN, int logC, int logR, int s) {
+    const size_t M = (size_t)1 << (logN - 1), C = (size_t)1 << logC, R = (size_t)1 << logR;
+    const size_t nblocks = R / kRowG;
+    Layout L;
+    size_t o = 0;
+    L.V = o; o = up256(o + M * sizeof(double2));
+    L.carry = o; o = up256(o + nblocks * C * sizeof(long long));
+    L.carry2 = o; o = up256(o + nblocks * C * sizeof(int));
+    L.ctl = o; o = up256(o + sizeof(LargeCtl));
+    L.qtwC = o; o = up256(o + (C / 4) * sizeof(double2));
+    L.qtwR = o; o = up256(o + (R / 4) * sizeof(double2));
+    L.tw1 = o; o = up256(o + ((size_t)1 << s) * sizeof(double2));
+    L.tw2 = o; o = up256(o + (M >> s) * sizeof(double2));
+    L.pos_of_c = o; o = up256(o + C * sizeof(int));
+    L.wA = o; o = up256(o + 2 * R * sizeof(double));
+    L.iwA = o; o = up256(o + 2 * R * sizeof(double));
+    L.sA = o; o = up256(o + 2 * R * sizeof(int));
+    L.wB = o; o = up256(o + C * sizeof(double));
+    L.iwB = o; o = up256(o + C * sizeof(double));
+    L.sB = o; o = up256(o + C * sizeof(int));
+    L.end = o;
+    return L;
+}
+
+int pos_of_freq_host(int log_l, int k) {
+    const int L = 1 << log_l, P = (log_l + 3) / 4;
+    const int RLAST = (log_l % 4 == 0) ? 16 : (1 << (log_l % 4));
+    const int klast = k / (L / RLAST);
+    int low = k % (L / RLAST), rest = 0;
+    for (int q = 0; q < P - 1; ++q) {
+        rest = (rest << 4) | (low & 15);
+        low >>= 4;
+    }
+    return rest * RLAST + klast;
+}
+
+// Copies `count` table entries produced by f(i) into the scratch at byte offset `off`, through
+// the static host stage in slices.
+template <class T, class F>
+cudaError_t put_table(unsigned char* dev, size_t off, size_t count, F f, cudaStream_t st) {
+    T* stage = reinterpret_cast<T*>(g_stage);
+    const size_t per = kStageBytes / sizeof(T);
+    for (size_t base = 0; base < count; base += per) {
+        const size_t n = count - base < per ? count - base : per;
+        for (size_t i = 0; i < n; ++i) stage[i] = f(base + i);
+        // pageable source: the copy has consumed the stage when the call returns
+        cudaError_t e = cudaMemcpyAsync(dev + off + base * sizeof(T), stage, n * sizeof(T),
+                                        cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return e;
+        e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+double2 omega(uint64_t period, uint64_t e) {
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    const long double ang = two_pi * (long double)(e % period) / (long double)period;
+    return make_double2((double)cosl(ang), -(double)sinl(ang));
+}
+
+}  // namespace
+
+}  // namespace llg
+
+using namespace llg;
+
+extern "C" int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* digits_out,
+                               double* max_err, void* stream) {
+    if (!digits_out) return set_error(LLG_E_ARG, "llg_run_noalloc: digits_out is null");
+    if (p < 3 || p % 2 == 0 || iters == 0)
+        return set_error(LLG_E_ARG, "llg_run_noalloc: p must be odd and >= 3, iters >= 1");
+    int logN = 0;
+    while ((1ull << logN) < n) ++logN;
+    if ((1ull << logN) != n || logN < 14 || logN > kNoAllocMaxLog)
+        return set_error(LLG_E_UNSUPPORTED,
+                         "llg_run_noalloc: n must be a power of two from 16384 to 65536 (its fixed "
+                         "640 KiB device array holds nothing larger)");
+    const uint64_t N = n, M = N / 2;
+    // same usability rule as the allocating two-pass path: at least log2(N)/4 + 3 bits per digit
+    if (4 * (p / N) < (uint64_t)logN + 12 || (p + N - 1) / N > 28)
+        return set_error(LLG_E_UNSUPPORTED, "llg_run_noalloc: length not usable for this p (bits per digit)");
+    const int logC = (logN <= 15) ? logN - 8 : 8;
+    const int logR = logN - 1 - logC;
+    const int C = 1 << logC, R = 1 << logR;
+    const int s = logC > (logN / 2) ? logC : (logN / 2);
+    const Layout L = layout(logN, logC, logR, s);
+    if (L.end > kNoAllocScratchBytes) return set_error(LLG_E_UNSUPPORTED, "llg_run_noalloc: state exceeds the array");
+
+    std::lock_guard<std::mutex> lk(g_noalloc_mx);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return LLG_E_NODEV;
+    if (!g_scratch_addr[dev]) {
+        void* ptr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr) return LLG_E_CUDA;
+        g_scratch_addr[dev] = static_cast<unsigned char*>(ptr);
+    }
+    unsigned char* base = g_scratch_addr[dev];
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = configure_large(logC, logR);
+    if (e != cudaSuccess) return LLG_E_CUDA;
+
+    // tables (exact integers and long-double rounded values, as the allocating path uses)
+    const long double Nl = (long double)N;
+#define PUT(T, off, cnt, expr)                                                          \
+    do {                                                                                \
+        e = put_table<T>(base, off, cnt, [&](size_t i) -> T { return expr; }, st);      \
+        if (e != cudaSuccess) return LLG_E_CUDA;                                        \
+    } while (0)
+    PUT(double2, L.qtwC, (size_t)C / 4, omega(C, i));
+    PUT(double2, L.qtwR, (size_t)R / 4, omega(R, i));
+    PUT(double2, L.tw1, (size_t)1 << s, omega(M, i));
+    PUT(double2, L.tw2, (size_t)(M >> s), omega(M, (uint64_t)i << s));
+    PUT(int, L.pos_of_c, (size_t)C, pos_of_freq_host(logC, (int)i));
+    auto sAj = [&](size_t j) { return (N - (uint64_t)(((unsigned __int128)j * p) % N)) % N; };
+    auto sBb = [&](size_t b) { return (N - (uint64_t)(((unsigned __int128)2 * R * b * p) % N)) % N; };
+    PUT(double, L.wA, (size_t)2 * R, (double)exp2l((long double)sAj(i) / Nl));
+    PUT(double, L.iwA, (size_t)2 * R, (double)exp2l(-(long double)sAj(i) / Nl));
+    PUT(int, L.sA, (size_t)2 * R, (int)sAj(i));
+    PUT(double, L.wB, (size_t)C, (double)exp2l((long double)sBb(i) / Nl));
+    PUT(double, L.iwB, (size_t)C, (double)(exp2l(-(long double)sBb(i) / Nl) / (4.0L * (long double)M)));
+    PUT(int, L.sB, (size_t)C, (int)sBb(i));
+#undef PUT
+
+    LargeArgs A;
+    std::memset(&A, 0, sizeof A);
+    A.V = reinterpret_cast<double2*>(base + L.V);
+    A.qtwC = reinterpret_cast<const double2*>(base + L.qtwC);
+    A.qtwR = reinterpret_cast<const double2*>(base + L.qtwR);
+    A.tw1 = reinterpret_cast<const double2*>(base + L.tw1);
+    A.tw2 = reinterpret_cast<const double2*>(base + L.tw2);
+    A.pos_of_c = reinterpret_cast<const int*>(base + L.pos_of_c);
+    A.wA = reinterpret_cast<const double*>(base + L.wA);
+    A.iwA = reinterpret_cast<const double*>(base + L.iwA);
+    A.sA = reinterpret_cast<const int*>(base + L.sA);
+    A.wB = reinterpret_cast<const double*>(base + L.wB);
+    A.iwB = reinterpret_cast<const double*>(base + L.iwB);
+    A.sB = reinterpret_cast<const int*>(base + L.sB);
+    A.carry = reinterpret_cast<long long*>(base + L.carry);
+    A.carry2 = reinterpret_cast<int*>(base + L.carry2);
+    A.ctl = reinterpret_cast<LargeCtl*>(base + L.ctl);
+    A.digits = digits_out;
+    A.errlog = nullptr;
+    A.errlog_len = 1;
+    A.dump = 0;
+    A.tw_shift = s;
+    A.C = C;
+    A.R = R;
+    A.nblocks = R / kRowG;
+    A.q = (int)(p >> logN);
+    A.rem = (int)(p & (N - 1));
+    A.logN = logN;
+
+    // s_0 = 4 as digits (the output buffer doubles as the INIT input), control block cleared
+    static const int32_t four = 4;
+    if (cudaMemsetAsync(digits_out, 0, N * sizeof(int32_t), st) != cudaSuccess) return LLG_E_CUDA;
+    if (cudaMemcpyAsync(digits_out, &four, sizeof four, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return LLG_E_CUDA;
+    if (cudaMemsetAsync(A.ctl, 0, sizeof(LargeCtl), st) != cudaSuccess) return LLG_E_CUDA;
+    if (launch_large_row(logC, LARGE_INIT, A, st) != cudaSuccess) return LLG_E_CUDA;
+    if (launch_large_col(logR, A, st) != cudaSuccess) return LLG_E_CUDA;
+    for (uint64_t k = 1; k < iters; ++k) {
+        if (launch_large_row(logC, LARGE_ITER, A, st) != cudaSuccess) return LLG_E_CUDA;
+        if (launch_large_col(logR, A, st) != cudaSuccess) return LLG_E_CUDA;
+    }
+    if (launch_large_row(logC, LARGE_FINAL, A, st) != cudaSuccess) return LLG_E_CUDA;
+    LargeCtl h;
+    if (cudaMemcpyAsync(&h, A.ctl, offsetof(LargeCtl, flags), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return LLG_E_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return LLG_E_CUDA;
+    double err;
+    std::memcpy(&err, &h.err_max, sizeof err);
+    if (max_err) *max_err = err;
+    if (h.timeout) return LLG_E_TIMEOUT;
+    return err > 0.4 ? LLG_E_ROUNDOFF : LLG_OK;
+}

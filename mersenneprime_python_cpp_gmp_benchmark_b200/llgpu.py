@@ -68,6 +68,7 @@ def lib() -> ctypes.CDLL:
         L.llg_measure_peak.argtypes = [ctypes.c_int, P(dbl)]
         L.llg_batch_device_ms.argtypes = [ctypes.c_void_p, P(ctypes.c_float)]
         L.llg_batch_destroy.argtypes = [ctypes.c_void_p]
+        L.llg_run_noalloc.argtypes = [u64, u64, u32, ctypes.c_void_p, P(dbl), ctypes.c_void_p]
         L.llg_test_create.argtypes = [u64, u32, P(ctypes.c_void_p)]
         L.llg_test_start.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.llg_test_iterate.argtypes = [ctypes.c_void_p, u64, ctypes.c_void_p]
@@ -238,6 +239,15 @@ class Test:
             self.close()
         except Exception:
             pass
+
+
+def run_noalloc(p, iters, n, digits_dev_ptr, stream=0):
+    """llg_run_noalloc: squarings without device allocation; digits land in the caller's device
+    buffer (n int32). Returns the worst round-off."""
+    err = ctypes.c_double()
+    _check(lib().llg_run_noalloc(p, iters, n, ctypes.c_void_p(digits_dev_ptr), ctypes.byref(err),
+                                 ctypes.c_void_p(stream or None)))
+    return err.value
 
 
 def residue_from_digits(p, n, digits):
