@@ -68,23 +68,14 @@ int device_ready(int* dev_out) {
     return LLG_OK;
 }
 
-// e^{-2 pi i r / M}, r < M/4, rounded once from long double.
-std::vector<double2> quarter_table(int log_m) {
-    const size_t M = (size_t)1 << log_m, Q = M / 4;
-    std::vector<double2> q(Q);
-    const long double two_pi = 6.283185307179586476925286766559005768L;
-    for (size_t r = 0; r < Q; ++r) {
-        long double a = two_pi * (long double)r / (long double)M;
-        q[r] = make_double2((double)cosl(a), -(double)sinl(a));
-    }
-    return q;
-}
+// e^{-2 pi i r / M}, r < M/4, rounded once from long double, stored at qpad(r).
+std::vector<double2> quarter_table(int log_m) { return padded_quarter_table((uint64_t)1 << log_m); }
 
 int get_qtw(int dev, int log_m, const double2** out) {
     std::lock_guard<std::mutex> lk(g_mx);
     DeviceTables& T = g_tables[dev];
     if (!T.qtw[log_m]) {
-        std::vector<double2> h = quarter_table(log_m);
+        std::vector<double2> h = quarter_table(log_m);  // padded layout (qpad)
         double2* d = nullptr;
         CK(cudaMalloc(&d, h.size() * sizeof(double2)));
         CK(cudaMemcpy(d, h.data(), h.size() * sizeof(double2), cudaMemcpyHostToDevice));

@@ -132,13 +132,18 @@ struct Dft<16, INV> {
     __device__ __forceinline__ static void run(double2* v) { DftSplit<4, 4, INV>::run(v); }
 };
 
-// Twiddle e^{-2 pi i x / M} (conjugated when inv) from a quarter-wave table
-// q[r] = e^{-2 pi i r / M}, r < M/4.  x in [0, M).
+// Quarter-wave tables are stored padded: entry r at qpad(r) = r + r/8, so the strided indices of
+// the radix passes (multiples of 16 and of small odd numbers) spread over the shared-memory banks.
+__host__ __device__ constexpr uint32_t qpad(uint32_t r) { return r + (r >> 3); }
+__host__ __device__ constexpr uint32_t qpad_len(uint32_t qm) { return qm + (qm >> 3) + 1; }
+
+// Twiddle e^{-2 pi i x / M} (conjugated when inv) from a padded quarter-wave table
+// q[qpad(r)] = e^{-2 pi i r / M}, r < M/4.  x in [0, M).
 template <int LOG_M>
 __device__ __forceinline__ double2 twiddle(const double2* __restrict__ q, uint32_t x, bool inv) {
     constexpr uint32_t QM = (1u << LOG_M) / 4;
     const uint32_t quad = (x / QM) & 3u;
-    double2 w = q[x % QM];
+    double2 w = q[qpad(x % QM)];
     // rotate by (-i)^quad
     double2 r;
     switch (quad) {

@@ -4,8 +4,9 @@
 // holds 16 values. Forward = decimation in frequency: natural order in (thread t holds element
 // t + T*i in v[i]), mixed-radix digit-reversed order out (thread t holds positions 16t + j in
 // v[j]; freq_of_pos / pos_of_freq translate). Inverse = the same passes retraced, back to natural
-// order, unscaled (x L). The exchange buffer is two padded double arrays (re, im) of
-// L + L/16 entries; phys() pads one slot per 16 so strided accesses spread over the banks.
+// order, unscaled (x L). The exchange buffer is one array of L + L/16 complex (16-byte) slots;
+// phys() pads one slot per 16, which keeps every pass's access pattern at the minimum of four
+// shared-memory wavefronts per warp access (at most five).
 #pragma once
 
 #include <cstdint>
@@ -14,24 +15,26 @@
 
 namespace llg {
 
-template <int LOG_M>
+// L = 2^LOG_M points, E = 2^LOG_E values per thread (radix-E passes, the last one RLAST).
+template <int LOG_M, int LOG_E = 4>
 struct SmallGeom {
     static constexpr int M = 1 << LOG_M;
     static constexpr int N = 2 * M;
-    static constexpr int E = 16;               // complex values per thread
-    static constexpr int T = M / E;            // threads per test
-    static constexpr int P = (LOG_M + 3) / 4;  // radix passes
-    static constexpr int RLAST = (LOG_M % 4 == 0) ? 16 : (1 << (LOG_M % 4));
-    static constexpr int PAD = M + M / 16;     // padded exchange array length (doubles)
-    static constexpr int W = (T + 31) / 32;    // warps
-    static __host__ __device__ constexpr int radix(int s) { return s == P - 1 ? RLAST : 16; }
-    static __host__ __device__ constexpr int len(int s) { return M >> (4 * s); }
+    static constexpr int LE = LOG_E;
+    static constexpr int E = 1 << LOG_E;                  // complex values per thread
+    static constexpr int T = M / E;                       // threads per transform
+    static constexpr int P = (LOG_M + LOG_E - 1) / LOG_E; // radix passes
+    static constexpr int RLAST = (LOG_M % LOG_E == 0) ? E : (1 << (LOG_M % LOG_E));
+    static constexpr int PAD = M + M / 16;                // padded exchange array length (slots)
+    static constexpr int W = (T + 31) / 32;               // warps
+    static __host__ __device__ constexpr int radix(int s) { return s == P - 1 ? RLAST : E; }
+    static __host__ __device__ constexpr int len(int s) { return M >> (LOG_E * s); }
     static __host__ __device__ constexpr int stride(int s) { return len(s) / radix(s); }
 };
 
 __device__ __forceinline__ int phys(int x) { return x + (x >> 4); }
 
-// Frequency index k of DIF output position pos (mixed radix 16,...,16,RLAST digit reversal).
+// Frequency index k of DIF output position pos (mixed radix E,...,E,RLAST digit reversal).
 template <class G>
 __device__ __forceinline__ int freq_of_pos(int pos) {
     int klast = pos % G::RLAST;
@@ -39,8 +42,8 @@ __device__ __forceinline__ int freq_of_pos(int pos) {
     int k = 0;
 #pragma unroll
     for (int s = 0; s < G::P - 1; ++s) {
-        k = (k << 4) | (rest & 15);
-        rest >>= 4;
+        k = (k << G::LE) | (rest & (G::E - 1));
+        rest >>= G::LE;
     }
     // rest digits were stored most-significant-first as k1^(0); the loop above reversed them
     return k + klast * (G::M / G::RLAST);
@@ -53,19 +56,30 @@ __device__ __forceinline__ int pos_of_freq(int k) {
     int rest = 0;
 #pragma unroll
     for (int s = 0; s < G::P - 1; ++s) {
-        rest = (rest << 4) | (low & 15);
-        low >>= 4;
+        rest = (rest << G::LE) | (low & (G::E - 1));
+        low >>= G::LE;
     }
     return rest * G::RLAST + klast;
 }
 
+// Barrier for the threads of one transform: the whole block, or a named barrier covering only the
+// transform's own warps (several independent transforms per block then do not wait on each other).
+struct CtaSync {
+    __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+struct NamedSync {
+    unsigned id, nthreads;  // id 1..15; nthreads a multiple of 32
+    __device__ __forceinline__ void operator()() const {
+        asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+    }
+};
+
 // Forward (INV=false) or inverse radix pass S on the register array v (E values).
 // Forward: load (S > 0), DFT, twiddle w_L^{n2 k1}, store (S < P-1).
 // Inverse: load (S < P-1), conj twiddle, inverse DFT, store (S > 0).
-template <class G, int S, bool INV, bool SYNC_BEFORE_STORE = false>
-__device__ __forceinline__ void radix_pass(double2 (&v)[G::E], double* __restrict__ sre,
-                                           double* __restrict__ sim,
-                                           const double2* __restrict__ qtw, int t) {
+template <class G, int S, bool INV, bool SYNC_BEFORE_STORE, class SYNC>
+__device__ __forceinline__ void radix_pass(double2 (&v)[G::E], double2* __restrict__ buf,
+                                           const double2* __restrict__ qtw, int t, const SYNC& sync) {
     constexpr int R = G::radix(S);
     constexpr int L = G::len(S);
     constexpr int ST = G::stride(S);
@@ -82,7 +96,7 @@ __device__ __forceinline__ void radix_pass(double2 (&v)[G::E], double* __restric
 #pragma unroll
             for (int n1 = 0; n1 < R; ++n1) {
                 const int x = phys(base + n1 * ST);
-                vv[n1] = make_double2(sre[x], sim[x]);
+                vv[n1] = buf[x];
             }
         }
         if constexpr (!INV) {
@@ -90,13 +104,13 @@ __device__ __forceinline__ void radix_pass(double2 (&v)[G::E], double* __restric
             if constexpr (ST > 1) {
 #pragma unroll
                 for (int k1 = 1; k1 < R; ++k1)
-                    vv[k1] = cmul(vv[k1], twiddle<G::LOG_M_>(qtw, (uint32_t)(n2 * k1) << (4 * S), false));
+                    vv[k1] = cmul(vv[k1], twiddle<G::LOG_M_>(qtw, (uint32_t)(n2 * k1) << (G::LE * S), false));
             }
         } else {
             if constexpr (ST > 1) {
 #pragma unroll
                 for (int k1 = 1; k1 < R; ++k1)
-                    vv[k1] = cmul(vv[k1], twiddle<G::LOG_M_>(qtw, (uint32_t)(n2 * k1) << (4 * S), true));
+                    vv[k1] = cmul(vv[k1], twiddle<G::LOG_M_>(qtw, (uint32_t)(n2 * k1) << (G::LE * S), true));
             }
             Dft<R, true>::run(vv);
         }
@@ -104,13 +118,12 @@ __device__ __forceinline__ void radix_pass(double2 (&v)[G::E], double* __restric
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1) {
                 const int x = phys(base + k1 * ST);
-                sre[x] = vv[k1].x;
-                sim[x] = vv[k1].y;
+                buf[x] = vv[k1];
             }
         }
     }
     if constexpr (STORE && SYNC_BEFORE_STORE) {
-        __syncthreads();
+        sync();
 #pragma unroll
         for (int h = 0; h < B; ++h) {
             const int beta = t * B + h;
@@ -119,35 +132,38 @@ __device__ __forceinline__ void radix_pass(double2 (&v)[G::E], double* __restric
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1) {
                 const int x = phys(base + k1 * ST);
-                sre[x] = v[h * R + k1].x;
-                sim[x] = v[h * R + k1].y;
+                buf[x] = v[h * R + k1];
             }
         }
     }
 }
 
-template <class G, int S>
-__device__ __forceinline__ void forward_from(double2 (&v)[G::E], double* sre, double* sim,
-                                             const double2* qtw, int t) {
+// Forward passes S .. P-1 (pass S loads from buf unless S == 0).
+template <class G, int S, class SYNC = CtaSync>
+__device__ __forceinline__ void forward_from(double2 (&v)[G::E], double2* buf, const double2* qtw,
+                                             int t, const SYNC& sync = SYNC()) {
     if constexpr (S < G::P) {
-        radix_pass<G, S, false>(v, sre, sim, qtw, t);
-        if constexpr (S < G::P - 1) __syncthreads();
-        forward_from<G, S + 1>(v, sre, sim, qtw, t);
+        radix_pass<G, S, false, false>(v, buf, qtw, t, sync);
+        if constexpr (S < G::P - 1) sync();
+        forward_from<G, S + 1, SYNC>(v, buf, qtw, t, sync);
     }
 }
 
-template <class G, int S>
-__device__ __forceinline__ void inverse_from(double2 (&v)[G::E], double* sre, double* sim,
-                                             const double2* qtw, int t) {
+// Inverse passes S down to 0, starting from registers. FIRST_SYNC: a barrier between the first
+// pass's arithmetic and its stores (needed when other threads may still read the positions it
+// overwrites, e.g. a partner read of the same buffer).
+template <class G, int S, bool FIRST_SYNC = true, class SYNC = CtaSync>
+__device__ __forceinline__ void inverse_from(double2 (&v)[G::E], double2* buf, const double2* qtw,
+                                             int t, const SYNC& sync = SYNC()) {
     if constexpr (S >= 0) {
-        radix_pass<G, S, true, S == G::P - 1>(v, sre, sim, qtw, t);
-        if constexpr (S > 0) __syncthreads();
-        inverse_from<G, S - 1>(v, sre, sim, qtw, t);
+        radix_pass<G, S, true, FIRST_SYNC && S == G::P - 1>(v, buf, qtw, t, sync);
+        if constexpr (S > 0) sync();
+        inverse_from<G, S - 1, false, SYNC>(v, buf, qtw, t, sync);
     }
 }
 
-template <int LOG_M_T>
-struct SmallG : SmallGeom<LOG_M_T> {
+template <int LOG_M_T, int LOG_E = 4>
+struct SmallG : SmallGeom<LOG_M_T, LOG_E> {
     static constexpr int LOG_M_ = LOG_M_T;
 };
 

@@ -16,6 +16,10 @@ bool large_length_supported(int log_n);
 int set_error(int code, const char* msg);  // records this thread's llg_last_error() text
 cudaError_t configure_large(int log_c, int log_r);
 std::vector<int> seed_digits(uint64_t n);
+// Quarter-wave table of an L-point FFT in the padded layout the kernels read (entry r at qpad(r)).
+std::vector<double2> padded_quarter_table(uint64_t L);
+// Value of slot i of that layout (zero in the padding slots).
+double2 padded_quarter_slot(uint64_t L, uint64_t i);
 
 struct LargeTest {
     uint64_t p = 0, M = 0;

@@ -35,7 +35,8 @@ cudaError_t launch_word(const SmallJob* jobs, int njobs, uint64_t* res, cudaStre
 
 // ---- two-pass engine (N = 2^16 .. 2^23): state resident in HBM ------------------------------
 
-constexpr int kRowG = 8;              // rows per row-pass block
+constexpr int kRowG = 4;              // rows per row-pass block
+constexpr int kLargeLogE = 4;         // log2 of the complex values per thread in the two-pass kernels
 constexpr int kLargeMaxBlocks = 1024; // row blocks (R / kRowG) supported by the control block
 
 struct LargeCtl {

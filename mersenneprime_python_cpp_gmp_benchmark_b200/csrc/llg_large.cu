@@ -8,12 +8,12 @@
 // lucaslehmer.cpp:282,289-310):
 //
 //   row pass (one block = kRowG consecutive rows, all C columns):
-//       conj twiddle w_M^{-ac}, inverse C-point FFT          (end of the previous squaring)
+//       inverse C-point FFT                                   (end of the previous squaring)
 //       unweight, round, max round-off, carry, "- 2"
-//       weight, forward C-point FFT, twiddle w_M^{ac}        (start of this squaring)
+//       weight, forward C-point FFT                           (start of this squaring)
 //   column pass (one block = the column pair c, C-c):
-//       forward R-point FFT, real-FFT split + pointwise square over the pair (k, M-k),
-//       inverse R-point FFT
+//       twiddle w_M^{ac}, forward R-point FFT, real-FFT split + pointwise square over the pair
+//       (k, M-k), inverse R-point FFT, twiddle w_M^{-ac}
 //
 // The state is stored column-slot-major (element (a, pos) at pos*R + a), so a row block reads
 // and writes kRowG contiguous complex values (128 bytes) per column slot and a column block reads
@@ -31,6 +31,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "llg_device.cuh"
 #include "llg_fft.cuh"
@@ -53,13 +54,15 @@ __device__ __forceinline__ double2 twiddle_M(const LargeArgs& A, uint32_t x, boo
 }  // namespace
 
 template <int LOG_C, int MODE>
-__global__ void __launch_bounds__(kRowG * (1 << LOG_C) / 16, 1) large_row(const LargeArgs A) {
-    using GC = SmallG<LOG_C>;
-    constexpr int C = GC::M, TR = GC::T, E = 16, G = kRowG, T = G * TR;
+__global__ void __launch_bounds__(kRowG * (1 << LOG_C) / (1 << kLargeLogE), 2) large_row(const LargeArgs A) {
+    using GC = SmallG<LOG_C, kLargeLogE>;
+    constexpr int C = GC::M, TR = GC::T, E = GC::E, G = kRowG, T = G * TR;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* bufs = reinterpret_cast<double*>(smem_raw);                  // G x (re, im) x PAD
-    double2* qtw = reinterpret_cast<double2*>(bufs + 2 * G * GC::PAD);   // C/4
-    long long* hin = reinterpret_cast<long long*>(qtw + C / 4);  // C: wrap carry into row 0 (hop 2)
+    constexpr int RS = GC::PAD + 1;  // row-buffer stride: odd, so the 8 rows of a slot hit 8 banks
+    double2* bufs = reinterpret_cast<double2*>(smem_raw);        // G exchange buffers of RS slots
+    double2* qtw = bufs + G * RS;                                  // padded quarter table (C-point)
+    constexpr int QL = (int)qpad_len(C / 4);
+    long long* hin = reinterpret_cast<long long*>(qtw + QL);      // C: wrap carry into row 0 (hop 2)
     long long* hc1 = hin + C;                                     // C: row R-2's carry-out (block 0)
     int* hin2 = reinterpret_cast<int*>(hc1 + C);                  // C: wrap carry into row 0 (hop 3)
     long long* carr = reinterpret_cast<long long*>(bufs);         // G x C hop-1 carry-outs (reuses bufs)
@@ -69,9 +72,12 @@ __global__ void __launch_bounds__(kRowG * (1 << LOG_C) / 16, 1) large_row(const 
     __shared__ unsigned s_epoch;
 
     const int t = threadIdx.x, rg = t / TR, tr = t % TR;
-    double* sre = bufs + rg * 2 * GC::PAD;
-    double* sim = sre + GC::PAD;
+    double2* buf = bufs + rg * RS;
     const int N = 1 << A.logN, R = A.R;
+    // each row's FFT exchanges wait only on that row's warps (named barrier 1 + rg)
+    using RowSync = typename std::conditional<(TR >= 32), NamedSync, CtaSync>::type;
+    RowSync gsync;
+    if constexpr (TR >= 32) gsync = NamedSync{1u + (unsigned)rg, (unsigned)TR};
 
     if (t == 0) {
         const unsigned ep = *reinterpret_cast<volatile unsigned*>(&A.ctl->epoch);
@@ -85,7 +91,7 @@ __global__ void __launch_bounds__(kRowG * (1 << LOG_C) / 16, 1) large_row(const 
         }
         s_err = 0ull;
     }
-    for (int k = t; k < C / 4; k += T) qtw[k] = A.qtwC[k];
+    for (int k = t; k < QL; k += T) qtw[k] = A.qtwC[k];
     __syncthreads();
     const int blk = s_blk;
     const unsigned ep = s_epoch;
@@ -118,12 +124,9 @@ __global__ void __launch_bounds__(kRowG * (1 << LOG_C) / 16, 1) large_row(const 
                 const int ah = R - 2 + hrow;
 #pragma unroll
                 for (int j = 0; j < E; ++j) {
-                    const int pos = tr * E + j;
-                    const double2 w = A.V[(size_t)pos * R + ah];
-                    const int c = freq_of_pos<GC>(pos);
-                    v[j] = cmul(w, twiddle_M(A, (uint32_t)ah * (uint32_t)c, true));
+                        v[j] = A.V[(size_t)(tr * E + j) * R + ah];
                 }
-                inverse_from<GC, GC::P - 1>(v, sre, sim, qtw, tr);
+                inverse_from<GC, GC::P - 1, false>(v, buf, qtw, tr, gsync);
                 const int h0 = __ldg(A.sA + 2 * ah), h1 = __ldg(A.sA + 2 * ah + 1);
                 const double ih0 = __ldg(A.iwA + 2 * ah), ih1 = __ldg(A.iwA + 2 * ah + 1);
 #pragma unroll
@@ -169,20 +172,13 @@ __global__ void __launch_bounds__(kRowG * (1 << LOG_C) / 16, 1) large_row(const 
 #pragma unroll
             for (int r = 0; r < G * C / T; ++r) {
                 const int qq = t + T * r, pos = qq / G, ra = qq % G;
-                const int x = phys(pos);
-                bufs[ra * 2 * GC::PAD + x] = tmp[r].x;
-                bufs[ra * 2 * GC::PAD + GC::PAD + x] = tmp[r].y;
+                bufs[ra * RS + phys(pos)] = tmp[r];
             }
         }
         __syncthreads();
 #pragma unroll
-        for (int j = 0; j < E; ++j) {
-            const int pos = tr * E + j;
-            const int x = phys(pos);
-            const int c = freq_of_pos<GC>(pos);
-            v[j] = cmul(make_double2(sre[x], sim[x]), twiddle_M(A, (uint32_t)a * (uint32_t)c, true));
-        }
-        inverse_from<GC, GC::P - 1>(v, sre, sim, qtw, tr);
+        for (int j = 0; j < E; ++j) v[j] = buf[phys(tr * E + j)];
+        inverse_from<GC, GC::P - 1, false>(v, buf, qtw, tr, gsync);
         __syncthreads();  // the exchange buffers become the carry arrays
 
         // ---- carry. Hop 1: unweight, round, round-off, two-digit chain per (row, column) from
@@ -307,33 +303,28 @@ __global__ void __launch_bounds__(kRowG * (1 << LOG_C) / 16, 1) large_row(const 
         v[i].x = i2d_shift(x0s[i]) * (wa0 * wb) * (o0 ? 0.5 : 1.0);
         v[i].y = i2d_shift(x1s[i]) * (wa1 * wb) * (o1 ? 0.5 : 1.0);
     }
-    forward_from<GC, 0>(v, sre, sim, qtw, tr);
+    forward_from<GC, 0>(v, buf, qtw, tr, gsync);
 #pragma unroll
-    for (int j = 0; j < E; ++j) {
-        const int pos = tr * E + j;
-        const int c = freq_of_pos<GC>(pos);
-        const double2 w = cmul(v[j], twiddle_M(A, (uint32_t)a * (uint32_t)c, false));
-        const int x = phys(pos);
-        sre[x] = w.x;
-        sim[x] = w.y;
-    }
+    for (int j = 0; j < E; ++j) buf[phys(tr * E + j)] = v[j];
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < G * C / T; ++r) {
         const int qq = t + T * r, pos = qq / G, ra = qq % G;
-        const int x = phys(pos);
-        A.V[(size_t)pos * R + a0 + ra] =
-            make_double2(bufs[ra * 2 * GC::PAD + x], bufs[ra * 2 * GC::PAD + GC::PAD + x]);
+        A.V[(size_t)pos * R + a0 + ra] = bufs[ra * RS + phys(pos)];
     }
 }
 
+// Column pass: one block owns the column pair (c, C-c), one half of its threads per column; the
+// real-FFT split reads the partner column's spectrum from the other half's exchange buffer.
+// Block 0 holds column 0 and block C/2 column C/2, each of which pairs with itself.
 template <int LOG_R>
-__global__ void __launch_bounds__(2 * (1 << LOG_R) / 16, 1) large_col(const LargeArgs A) {
-    using GR = SmallG<LOG_R>;
-    constexpr int R = GR::M, TC = GR::T, E = 16;
+__global__ void __launch_bounds__(2 * (1 << LOG_R) / (1 << kLargeLogE), 1) large_col(const LargeArgs A) {
+    using GR = SmallG<LOG_R, kLargeLogE>;
+    constexpr int R = GR::M, TC = GR::T, E = GR::E;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* bufs = reinterpret_cast<double*>(smem_raw);                 // 2 x (re, im) x PAD
-    double2* qtw = reinterpret_cast<double2*>(bufs + 4 * GR::PAD);       // R/4
+    double2* bufs = reinterpret_cast<double2*>(smem_raw);  // 2 exchange buffers of PAD slots
+    double2* qtw = bufs + 2 * GR::PAD;                       // padded quarter table (R-point)
+    constexpr int QL = (int)qpad_len(R / 4);
     const int t = threadIdx.x, half = t / TC, tc = t % TC;
     const int C = A.C;
     const int cb = blockIdx.x;  // 0 .. C/2
@@ -341,23 +332,28 @@ __global__ void __launch_bounds__(2 * (1 << LOG_R) / 16, 1) large_col(const Larg
     const bool self = (c1 == c2);
     const bool active = !(self && half == 1);
     const int c = half ? c2 : c1;
-    double* sre = bufs + half * 2 * GR::PAD;
-    double* sim = sre + GR::PAD;
-    const double* pre = self ? sre : bufs + (1 - half) * 2 * GR::PAD;  // partner column
-    const double* pim = pre + GR::PAD;
-    for (int k = t; k < R / 4; k += 2 * TC) qtw[k] = A.qtwR[k];
+    double2* buf = bufs + half * GR::PAD;
+    const double2* pbuf = self ? buf : bufs + (1 - half) * GR::PAD;  // partner column
+    // each column's FFT exchanges wait only on that column's warps (named barrier 1 + half)
+    using ColSync = typename std::conditional<(TC >= 32), NamedSync, CtaSync>::type;
+    ColSync gsync;
+    if constexpr (TC >= 32) gsync = NamedSync{1u + (unsigned)half, (unsigned)TC};
+    for (int k = t; k < QL; k += 2 * TC) qtw[k] = A.qtwR[k];
     double2* col = A.V + (size_t)__ldg(A.pos_of_c + c) * R;
+    // four-step twiddle w_M^{a c} for a = tc + TC i, factored as w_M^{c tc} * w_M^{c TC i}: one
+    // value per thread and an E-entry table per column (broadcast reads)
+    double2* ptab = qtw + QL + half * E;
+    for (int i = tc; i < E; i += TC) ptab[i] = twiddle_M(A, (uint32_t)c * (uint32_t)(TC * i), false);
+    const double2 q = twiddle_M(A, (uint32_t)c * (uint32_t)tc, false);
     double2 v[E];
 #pragma unroll
     for (int i = 0; i < E; ++i) v[i] = active ? col[tc + TC * i] : make_double2(0.0, 0.0);
     __syncthreads();
-    forward_from<GR, 0>(v, sre, sim, qtw, tc);
 #pragma unroll
-    for (int j = 0; j < E; ++j) {
-        const int x = phys(tc * E + j);
-        sre[x] = v[j].x;
-        sim[x] = v[j].y;
-    }
+    for (int i = 0; i < E; ++i) v[i] = cmul(v[i], cmul(q, ptab[i]));
+    forward_from<GR, 0>(v, buf, qtw, tc, gsync);
+#pragma unroll
+    for (int j = 0; j < E; ++j) buf[phys(tc * E + j)] = v[j];
     __syncthreads();
     const double2 wc = __ldg(A.tw1 + c);  // w_M^c
 #pragma unroll
@@ -365,32 +361,34 @@ __global__ void __launch_bounds__(2 * (1 << LOG_R) / 16, 1) large_col(const Larg
         const int d = freq_of_pos<GR>(tc * E + j);
         const int dp = (c == 0) ? ((R - d) & (R - 1)) : (R - 1 - d);
         const int xp = phys(pos_of_freq<GR>(dp));
-        const double2 Av = v[j], Bc = make_double2(pre[xp], -pim[xp]);  // conj(U_{M-k})
+        const double2 Av = v[j], Bc = conj2(pbuf[xp]);  // conj(U_{M-k})
         const double2 s = cadd(Av, Bc), dd = csub(Av, Bc);
         const double2 a3 = make_double2(3.0 * Av.x - Bc.x, 3.0 * Av.y - Bc.y);
         const double2 d2 = make_double2((dd.x - dd.y) * (dd.x + dd.y), 2.0 * dd.x * dd.y);
         const double2 w = cmul(wc, twiddle<LOG_R>(qtw, (uint32_t)d, false));  // w_M^{c + C d}
         v[j] = csub(cmul(a3, s), cmul(w, d2));
     }
-    inverse_from<GR, GR::P - 1>(v, sre, sim, qtw, tc);
+    __syncthreads();  // partner reads done before either column overwrites its buffer
+    inverse_from<GR, GR::P - 1, false>(v, buf, qtw, tc, gsync);
     if (active) {
+        const double2 q2 = twiddle_M(A, (uint32_t)c * (uint32_t)tc, false);  // recomputed: frees registers
 #pragma unroll
-        for (int i = 0; i < E; ++i) col[tc + TC * i] = v[i];
+        for (int i = 0; i < E; ++i) col[tc + TC * i] = cmulc(v[i], cmul(q2, ptab[i]));
     }
     if (cb == 0 && t == 0) atomicAdd(&A.ctl->epoch, 1u);
 }
 
 template <int LOG_C>
 static size_t row_smem() {
-    using GC = SmallGeom<LOG_C>;
-    return sizeof(double) * 2 * kRowG * GC::PAD + sizeof(double2) * (GC::M / 4) + 2 * sizeof(long long) * GC::M +
-           sizeof(int) * GC::M;
+    using GC = SmallGeom<LOG_C, kLargeLogE>;
+    return sizeof(double2) * kRowG * (GC::PAD + 1) + sizeof(double2) * qpad_len(GC::M / 4) +
+           2 * sizeof(long long) * GC::M + sizeof(int) * GC::M;
 }
 
 template <int LOG_R>
 static size_t col_smem() {
-    using GR = SmallGeom<LOG_R>;
-    return sizeof(double) * 4 * GR::PAD + sizeof(double2) * (GR::M / 4);
+    using GR = SmallGeom<LOG_R, kLargeLogE>;
+    return sizeof(double2) * 2 * GR::PAD + sizeof(double2) * qpad_len(GR::M / 4) + sizeof(double2) * 2 * GR::E;
 }
 
 template <int LOG_C, int MODE>
@@ -407,13 +405,13 @@ static cudaError_t col_attr() {
 
 template <int LOG_C, int MODE>
 static cudaError_t row_t(const LargeArgs& a, cudaStream_t st) {
-    large_row<LOG_C, MODE><<<a.nblocks, kRowG * (1 << LOG_C) / 16, row_smem<LOG_C>(), st>>>(a);
+    large_row<LOG_C, MODE><<<a.nblocks, kRowG * (1 << LOG_C) / (1 << kLargeLogE), row_smem<LOG_C>(), st>>>(a);
     return cudaGetLastError();
 }
 
 template <int LOG_R>
 static cudaError_t col_t(const LargeArgs& a, cudaStream_t st) {
-    large_col<LOG_R><<<a.C / 2 + 1, 2 * (1 << LOG_R) / 16, col_smem<LOG_R>(), st>>>(a);
+    large_col<LOG_R><<<a.C / 2 + 1, 2 * (1 << LOG_R) / (1 << kLargeLogE), col_smem<LOG_R>(), st>>>(a);
     return cudaGetLastError();
 }
 

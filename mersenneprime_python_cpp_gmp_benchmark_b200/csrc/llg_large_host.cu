@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/llgpu.h"
+#include "llg_device.cuh"
 #include "llg_host.h"
 #include "llg_internal.h"
 
@@ -20,15 +21,18 @@ namespace llg {
 
 namespace {
 
-// mixed-radix (16, ..., 16, RLAST) digit reversal of the L-point FFT (host copy of pos_of_freq)
+// column slot of row-FFT frequency k
 int host_pos_of_freq(int log_l, int k) {
-    const int L = 1 << log_l, P = (log_l + 3) / 4;
-    const int RLAST = (log_l % 4 == 0) ? 16 : (1 << (log_l % 4));
+    // digit reversal of the row FFT's output positions (radix 2^kLargeLogE passes, the last one
+    // RLAST): host copy of pos_of_freq for SmallGeom<log_l, kLargeLogE>
+    const int LE = kLargeLogE, E = 1 << LE;
+    const int L = 1 << log_l, P = (log_l + LE - 1) / LE;
+    const int RLAST = (log_l % LE == 0) ? E : (1 << (log_l % LE));
     const int klast = k / (L / RLAST);
     int low = k % (L / RLAST), rest = 0;
-    for (int s = 0; s < P - 1; ++s) {
-        rest = (rest << 4) | (low & 15);
-        low >>= 4;
+    for (int q = 0; q < P - 1; ++q) {
+        rest = (rest << LE) | (low & (E - 1));
+        low >>= LE;
     }
     return rest * RLAST + klast;
 }
@@ -44,6 +48,28 @@ std::vector<double2> omega_table(uint64_t period, uint64_t count, uint64_t step)
     }
     return t;
 }
+
+template <class T>
+cudaError_t upload(T** d, const std::vector<T>& h);
+
+}  // namespace
+
+double2 padded_quarter_slot(uint64_t L, uint64_t i) {
+    if (i % 9 == 8) return make_double2(0.0, 0.0);
+    const uint64_t r = 8 * (i / 9) + (i % 9);
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    const long double ang = two_pi * (long double)r / (long double)L;
+    return make_double2((double)cosl(ang), -(double)sinl(ang));
+}
+
+std::vector<double2> padded_quarter_table(uint64_t L) {
+    const uint64_t n = qpad_len((uint32_t)(L / 4));
+    std::vector<double2> t(n);
+    for (uint64_t i = 0; i < n; ++i) t[i] = padded_quarter_slot(L, i);
+    return t;
+}
+
+namespace {
 
 template <class T>
 cudaError_t upload(T** d, const std::vector<T>& h) {
@@ -77,8 +103,8 @@ cudaError_t LargeTest::init(uint64_t p_, int log_n) {
     cudaError_t e;
     if ((e = configure_large(logC, logR))) return e;
     // tables
-    if ((e = upload(&qtwC, omega_table(C, C / 4, 1)))) return e;
-    if ((e = upload(&qtwR, omega_table(R, R / 4, 1)))) return e;
+    if ((e = upload(&qtwC, padded_quarter_table(C)))) return e;
+    if ((e = upload(&qtwR, padded_quarter_table(R)))) return e;
     if ((e = upload(&tw1, omega_table(M, 1ull << s, 1)))) return e;
     if ((e = upload(&tw2, omega_table(M, M >> s, 1ull << s)))) return e;
     std::vector<int> pc(C);

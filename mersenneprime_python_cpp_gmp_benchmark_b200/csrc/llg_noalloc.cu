@@ -30,6 +30,7 @@
 #include <mutex>
 
 #include "../../include/llgpu.h"
+#include "llg_device.cuh"
 #include "llg_host.h"
 #include "llg_internal.h"
 
@@ -67,8 +68,8 @@ Layout layout(int logN, int logC, int logR, int s) {
     L.carry = o; o = up256(o + nblocks * C * sizeof(long long));
     L.carry2 = o; o = up256(o + nblocks * C * sizeof(int));
     L.ctl = o; o = up256(o + sizeof(LargeCtl));
-    L.qtwC = o; o = up256(o + (C / 4) * sizeof(double2));
-    L.qtwR = o; o = up256(o + (R / 4) * sizeof(double2));
+    L.qtwC = o; o = up256(o + qpad_len((uint32_t)(C / 4)) * sizeof(double2));
+    L.qtwR = o; o = up256(o + qpad_len((uint32_t)(R / 4)) * sizeof(double2));
     L.tw1 = o; o = up256(o + ((size_t)1 << s) * sizeof(double2));
     L.tw2 = o; o = up256(o + (M >> s) * sizeof(double2));
     L.pos_of_c = o; o = up256(o + C * sizeof(int));
@@ -83,13 +84,16 @@ Layout layout(int logN, int logC, int logR, int s) {
 }
 
 int pos_of_freq_host(int log_l, int k) {
-    const int L = 1 << log_l, P = (log_l + 3) / 4;
-    const int RLAST = (log_l % 4 == 0) ? 16 : (1 << (log_l % 4));
+    // digit reversal of the row FFT's output positions (radix 2^kLargeLogE passes, the last one
+    // RLAST): host copy of pos_of_freq for SmallGeom<log_l, kLargeLogE>
+    const int LE = kLargeLogE, E = 1 << LE;
+    const int L = 1 << log_l, P = (log_l + LE - 1) / LE;
+    const int RLAST = (log_l % LE == 0) ? E : (1 << (log_l % LE));
     const int klast = k / (L / RLAST);
     int low = k % (L / RLAST), rest = 0;
     for (int q = 0; q < P - 1; ++q) {
-        rest = (rest << 4) | (low & 15);
-        low >>= 4;
+        rest = (rest << LE) | (low & (E - 1));
+        low >>= LE;
     }
     return rest * RLAST + klast;
 }
@@ -168,8 +172,8 @@ extern "C" int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* 
         e = put_table<T>(base, off, cnt, [&](size_t i) -> T { return expr; }, st);      \
         if (e != cudaSuccess) return LLG_E_CUDA;                                        \
     } while (0)
-    PUT(double2, L.qtwC, (size_t)C / 4, omega(C, i));
-    PUT(double2, L.qtwR, (size_t)R / 4, omega(R, i));
+    PUT(double2, L.qtwC, (size_t)qpad_len((uint32_t)C / 4), padded_quarter_slot(C, i));
+    PUT(double2, L.qtwR, (size_t)qpad_len((uint32_t)R / 4), padded_quarter_slot(R, i));
     PUT(double2, L.tw1, (size_t)1 << s, omega(M, i));
     PUT(double2, L.tw2, (size_t)(M >> s), omega(M, (uint64_t)i << s));
     PUT(int, L.pos_of_c, (size_t)C, pos_of_freq_host(logC, (int)i));

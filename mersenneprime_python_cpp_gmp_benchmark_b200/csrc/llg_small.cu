@@ -41,10 +41,10 @@ __global__ void __launch_bounds__(SmallGeom<LOG_M>::T, (SmallGeom<LOG_M>::T < 32
     using G = SmallG<LOG_M>;
     constexpr int M = G::M, N = G::N, E = G::E, T = G::T, W = G::W;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* sre = reinterpret_cast<double*>(smem_raw);
-    double* sim = sre + G::PAD;
-    double2* qtw = reinterpret_cast<double2*>(sim + G::PAD);     // M/4 entries
-    double* wB = reinterpret_cast<double*>(qtw + (M / 4 > 0 ? M / 4 : 1));
+    double2* buf = reinterpret_cast<double2*>(smem_raw);          // exchange buffer, PAD slots
+    double2* qtw = buf + G::PAD;                                   // padded quarter table
+    constexpr int QL = (int)qpad_len(M / 4);
+    double* wB = reinterpret_cast<double*>(qtw + QL);
     double* iwB = wB + E;
     int* sB = reinterpret_cast<int*>(iwB + E);
     long long* cbuf = reinterpret_cast<long long*>(sB + E + (E & 1 ? 1 : 0) + 2);  // W * E
@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(SmallGeom<LOG_M>::T, (SmallGeom<LOG_M>::T < 32
     const int q = (int)(p >> (LOG_M + 1));          // p / N
     const int rem = (int)(p & (uint64_t)(N - 1));   // p % N
 
-    for (int k = t; k < M / 4; k += blockDim.x) qtw[k] = qtw_g[k];
+    for (int k = t; k < QL; k += blockDim.x) qtw[k] = qtw_g[k];
     for (int i = t; i < E; i += T) {
         // digit j = 2m + e with m = t + T*i: s_j = (sA(t,e) + sB(i)) mod N
         const uint64_t s = (uint64_t)(N - (int)(((uint64_t)2 * T * i * p) & (uint64_t)(N - 1))) &
@@ -99,14 +99,13 @@ __global__ void __launch_bounds__(SmallGeom<LOG_M>::T, (SmallGeom<LOG_M>::T < 32
     int x0s[E], x1s[E];
 
     for (;;) {
-        forward_from<G, 0>(v, sre, sim, qtw, t);
+        forward_from<G, 0>(v, buf, qtw, t);
         // pair (k, M-k): real-FFT split + square, result scaled by 4 (folded into iwB)
         if (active) {
 #pragma unroll
             for (int j = 0; j < E; ++j) {
                 const int x = phys(t * E + j);
-                sre[x] = v[j].x;
-                sim[x] = v[j].y;
+                buf[x] = v[j];
             }
         }
         __syncthreads();
@@ -116,7 +115,7 @@ __global__ void __launch_bounds__(SmallGeom<LOG_M>::T, (SmallGeom<LOG_M>::T < 32
                 const int k = freq_of_pos<G>(t * E + j);
                 const int kp = (M - k) & (M - 1);
                 const int x = phys(pos_of_freq<G>(kp));
-                const double2 A = v[j], Bc = make_double2(sre[x], -sim[x]);  // conj(U_{M-k})
+                const double2 A = v[j], Bc = conj2(buf[x]);  // conj(U_{M-k})
                 const double2 s = cadd(A, Bc), d = csub(A, Bc);
                 const double2 a3 = make_double2(3.0 * A.x - Bc.x, 3.0 * A.y - Bc.y);
                 const double2 d2 = make_double2((d.x - d.y) * (d.x + d.y), 2.0 * d.x * d.y);
@@ -124,7 +123,7 @@ __global__ void __launch_bounds__(SmallGeom<LOG_M>::T, (SmallGeom<LOG_M>::T < 32
                 v[j] = csub(cmul(a3, s), cmul(w, d2));
             }
             // the first inverse pass stores only after a barrier (partners may still be reading)
-            inverse_from<G, G::P - 1>(v, sre, sim, qtw, t);
+            inverse_from<G, G::P - 1>(v, buf, qtw, t);
         }
 
         // unweight, round, error, local carry (even -> odd digit); the carry-out of column i goes
@@ -327,8 +326,8 @@ cudaError_t launch_word(const SmallJob* jobs, int njobs, uint64_t* res, cudaStre
 template <int LOG_M>
 static size_t small_smem_bytes() {
     using G = SmallGeom<LOG_M>;
-    size_t b = 2 * sizeof(double) * G::PAD;
-    b += sizeof(double2) * (G::M / 4 > 0 ? G::M / 4 : 1);
+    size_t b = sizeof(double2) * G::PAD;
+    b += sizeof(double2) * qpad_len(G::M / 4);
     b += 2 * sizeof(double) * G::E + sizeof(int) * (G::E + (G::E & 1 ? 1 : 0) + 2);
     b += sizeof(long long) * G::W * G::E + 2 * sizeof(unsigned long long);
     return b;
