@@ -1,20 +1,20 @@
 #!/usr/bin/env python3
 """Benchmark of the B200 Lucas-Lehmer engine; prints ONE JSON line (rank 0).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload range|...] [--impl b200|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload big|range] [--impl b200|reference]
 
-Workloads (synthetic inputs are the exponents themselves, from the sieve; s_0 = 4):
+Workloads (synthetic inputs: the exponents themselves, s_0 = 4; no dataset exists for this path):
+  big     (default) p = 136,279,841 on the two-pass FP64 IBDWT engine at N = 2^23; one step = 1000
+          squarings. metric: us per Lucas-Lehmer iteration (lower is better). value: CUDA events on
+          the launch stream, the 64 MiB state resident on the device, L2 flushed between steps.
+          e2e: lucaslehmer.fft_res64_after(p, 2000) -- tables, upload of s_0, squarings, digits
+          back, exact residue on the host -- per squaring.
   range   every prime p <= 100,001 (9,592 Lucas-Lehmer tests, 28 Mersenne hits), batched whole-test
           kernels bucketed by transform length. One step = every test run to completion.
-          metric: tests/s (higher is better).
-
-value: tests/s with the job lists already resident on the device (CUDA events recorded on the
-launch stream around each step; the L2 is flushed with a 512 MiB write between steps).
-e2e:   the same metric through the reference-facing call lucaslehmer_cuda.lucas_lehmer_batch(),
-       host lists in, (p, is_prime, seconds, res64) out, every host<->device copy and the exact
-       residue rebuild inside the timed region.
+          metric: tests/s. e2e: lucaslehmer_cuda.lucas_lehmer_batch() on the host list.
 --impl reference: the reference's own CPU engine (its lucaslehmer.cpp compiled unchanged into
-oracle/_ref/, GMP engine) on the host cores, on a bounded stratified sample of the same workload.
+oracle/_ref/) on the host cores for the same metric: bench_square at p = 136,279,841 (big) or a
+stratified sample of the range (range).
 """
 from __future__ import annotations
 
@@ -316,22 +316,32 @@ def bench_big(args, rank, world):
 
 
 def cpu_baseline_big(threads):
-    """Reference GMP engine (oracle/_ref) per-iteration time at p = 136,279,841: one full-size
-    squaring timed as gmp_res64_after(p, 29) - gmp_res64_after(p, 27) (s_k fills p bits by k~27)."""
+    """Reference CPU time per Lucas-Lehmer squaring at p = 136,279,841, from the reference's own
+    squaring micro-benchmark bench_square(bits, iters, depth) (lucaslehmer.cpp:181-205; GMP mpz
+    square of a p-bit number, plain and with the reference's 9-thread Karatsuba split), compiled
+    unchanged into oracle/_ref. The best of the two is the reported value."""
     from oracle import oracle
     ref = oracle.reference_module()
-    kind = "reference" if ref is not None else "port"
-    f = (lambda k: ref.gmp_res64_after(BIG_P, k)) if ref else (lambda k: oracle.ll_gmp(BIG_P, k))
-    t0 = time.perf_counter()
-    f(27)
-    t1 = time.perf_counter()
-    f(30)
-    t2 = time.perf_counter()
-    per = ((t2 - t1) - (t1 - t0)) / 3.0
-    return {"value": round(per * 1e6, 1), "unit": "us/iteration", "cores": 1, "kind": kind,
-            "sample": "reference GMP engine (lucas_lehmer_n via gmp_res64_after), p=136,279,841: "
-                      "(time of 30 squarings - time of 27) / 3, i.e. full-size squarings; one core "
-                      "(the reference's engine is single-threaded per test)"}
+    if ref is None:  # the oracle's GMP restatement: one full-size squaring by difference
+        t0 = time.perf_counter()
+        oracle.ll_gmp(BIG_P, 27)
+        t1 = time.perf_counter()
+        oracle.ll_gmp(BIG_P, 29)
+        t2 = time.perf_counter()
+        per = ((t2 - t1) - (t1 - t0)) / 2.0
+        return {"value": round(per * 1e6, 1), "unit": "us/iteration", "cores": 1, "kind": "port",
+                "sample": "oracle GMP restatement, p=136,279,841, (t(29) - t(27)) / 2 squarings"}
+    plain = ref.bench_square(BIG_P, 2, 0)
+    depth = 2 if threads >= 9 else (1 if threads >= 3 else 0)
+    split = ref.bench_square(BIG_P, 2, depth) if depth else float("inf")
+    best = min(plain, split)
+    return {"value": round(best * 1e6, 1), "unit": "us/iteration",
+            "cores": {0: 1, 1: 3, 2: 9}[depth] if best == split else 1, "kind": "reference",
+            "plain_1core_us": round(plain * 1e6, 1),
+            "split_us": None if split == float("inf") else round(split * 1e6, 1), "split_depth": depth,
+            "sample": "reference bench_square(136279841, iters=2, depth 0 and 2): seconds per "
+                      "squaring of a 136,279,841-bit number (GMP; depth 2 = the reference's 9-thread "
+                      "Karatsuba split), the mod 2^p-1 shift-and-add (~1% of a squaring) not included"}
 
 
 def cpu_baseline_range(threads, budget_s=20.0):
@@ -376,17 +386,22 @@ def main():
             return 0
         t0 = time.perf_counter()
         vals = []
-        for _ in range(args.warmup):
-            pass  # the reference engine has no warm-up state; warm-up steps are not repeated on CPU
+        # the reference's CPU engine keeps no state between steps: warm-up steps are not repeated
         for _ in range(args.steps):
-            vals.append(cpu_baseline_range(threads, budget_s=15.0))
+            vals.append(cpu_baseline_range(threads, budget_s=15.0) if args.workload == "range"
+                        else cpu_baseline_big(threads))
         v = statistics.median(x["value"] for x in vals)
-        line = {"metric": METRIC_RANGE, "value": v, "unit": "tests/s", "n_gpus": args.gpus,
-                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-                "scaling": "strong", "vs_baseline": None, "dtype": "int64 (GMP limbs)", "data": "synthetic",
-                "config": {"workload": "range p<=100001 (9592 LL tests)"}, "impl": "reference",
-                "cpu_baseline": vals[-1], "e2e": {"value": v, "unit": "tests/s", "h2d_bytes_per_step": 0,
-                                                   "d2h_bytes_per_step": 0},
+        if args.workload == "range":
+            metric, unit, hib, scaling = METRIC_RANGE, "tests/s", True, "strong"
+            cfg = {"workload": "range p<=100001 (9592 LL tests)"}
+        else:
+            metric, unit, hib, scaling = METRIC_BIG, "us/iteration", False, "weak"
+            cfg = {"workload": "p=136,279,841, one Lucas-Lehmer squaring (reference GMP engine)"}
+        line = {"metric": metric, "value": v, "unit": unit, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": hib,
+                "scaling": scaling, "vs_baseline": None, "dtype": "int64 (GMP limbs)", "data": "synthetic",
+                "config": cfg, "impl": "reference", "cpu_baseline": vals[-1],
+                "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                 "ms_per_step": round(1e3 * (time.perf_counter() - t0) / max(1, args.steps), 1)}
         print(json.dumps(line))
         return 0

@@ -20,6 +20,10 @@
 
 namespace {
 
+// padded layout of the NTT quarter tables (same as gl::qpad8 in llg_ntt.cuh)
+constexpr uint32_t gl_qpad8(uint32_t r) { return r + (r >> 4); }
+constexpr uint32_t gl_qpad8_len(uint32_t qm) { return qm + (qm >> 4) + 1; }
+
 using namespace llg;
 
 thread_local std::string t_last_error;
@@ -52,8 +56,43 @@ constexpr int kSmallLogMax = 13;  // N = 8192
 // ---- device tables ------------------------------------------------------------------------
 
 struct DeviceTables {
-    double2* qtw[kSmallLogMax + 1] = {};  // quarter-wave twiddles of the M = N/2 point FFT
+    double2* qtw[kSmallLogMax + 1] = {};   // quarter-wave twiddles of the M = N/2 point FFT
+    uint64_t* nqtw[kSmallLogMax + 1] = {}; // NTT: padded quarter table of the N-point transform
+    NttConst nk[kSmallLogMax + 1] = {};
 };
+
+// ---- Goldilocks arithmetic on the host (tables): cuda/ll_ntt.cu:42-44, 182-195 ---------------
+
+constexpr uint64_t kGQ = 0xFFFFFFFF00000001ull;
+uint64_t hmul(uint64_t a, uint64_t b) { return (uint64_t)(((unsigned __int128)a * b) % kGQ); }
+uint64_t hpow(uint64_t a, uint64_t e) {
+    uint64_t r = 1;
+    a %= kGQ;
+    while (e) {
+        if (e & 1) r = hmul(r, a);
+        a = hmul(a, a);
+        e >>= 1;
+    }
+    return r;
+}
+uint64_t hinv(uint64_t a) { return hpow(a, kGQ - 2); }
+
+// w_N = 7^((q-1)/N) and an N-th root of 2 from a primitive (192 N)-th root (2 has order 192)
+bool ntt_constants(int log_n, uint64_t& omega, NttConst& K) {
+    const uint64_t N = 1ull << log_n;
+    omega = hpow(7, (kGQ - 1) / N);
+    const uint64_t om = hpow(7, (kGQ - 1) / (192 * N)), r192 = hpow(om, N);
+    uint64_t pw = 1, s = 0;
+    for (; s < 192; ++s) {
+        if (pw == 2) break;
+        pw = hmul(pw, r192);
+    }
+    if (s == 192) return false;
+    K.root2 = hpow(om, s);
+    K.inv_root2 = hinv(K.root2);
+    K.invN = hinv(N % kGQ);
+    return true;
+}
 std::map<int, DeviceTables> g_tables;  // per device ordinal
 
 int device_ready(int* dev_out) {
@@ -82,6 +121,31 @@ int get_qtw(int dev, int log_m, const double2** out) {
         T.qtw[log_m] = d;
     }
     *out = T.qtw[log_m];
+    return LLG_OK;
+}
+
+int get_ntt(int dev, int log_n, const uint64_t** qtw, NttConst* K) {
+    std::lock_guard<std::mutex> lk(g_mx);
+    DeviceTables& T = g_tables[dev];
+    if (!T.nqtw[log_n]) {
+        uint64_t omega;
+        NttConst k;
+        if (!ntt_constants(log_n, omega, k)) return fail(LLG_E_UNSUPPORTED, "no N-th root of 2 for N=2^%d", log_n);
+        const uint32_t QL = (1u << log_n) / 4;
+        std::vector<uint64_t> h(gl_qpad8_len(QL), 0ull);
+        uint64_t w = 1;
+        for (uint32_t r = 0; r < QL; ++r) {
+            h[gl_qpad8(r)] = w;
+            w = hmul(w, omega);
+        }
+        uint64_t* d = nullptr;
+        CK(cudaMalloc(&d, h.size() * sizeof(uint64_t)));
+        CK(cudaMemcpy(d, h.data(), h.size() * sizeof(uint64_t), cudaMemcpyHostToDevice));
+        T.nqtw[log_n] = d;
+        T.nk[log_n] = k;
+    }
+    *qtw = T.nqtw[log_n];
+    *K = T.nk[log_n];
     return LLG_OK;
 }
 
@@ -123,6 +187,24 @@ uint32_t fp64_length(uint64_t p, double bpw) {
         const uint64_t N = 1ull << l;
         if ((double)p / (double)N <= bpw && fp64_length_usable(p, N)) return (uint32_t)N;
     }
+    return 0;
+}
+
+// NTT: exact while every convolution output stays below q/2, i.e. ceil(p/N) <= (63 - log2 N)/2
+// (cuda/ll_ntt.cu:172-175); the same bits-per-digit floor as the FP64 engines keeps the four-hop
+// carry balanced.
+constexpr int kNttLogMin = 6;  // N = 64, the reference's shortest NTT (cuda/ll_ntt.cu:177)
+
+bool ntt_length_usable(uint64_t p, uint64_t n) {
+    const int l = ilog2_exact(n);
+    if (l < kNttLogMin || l > kSmallLogMax) return false;
+    return (p + n - 1) / n <= (uint64_t)((63 - l) / 2) && 4 * (p / n) >= (uint64_t)l + 12;
+}
+
+uint32_t ntt_len(uint64_t p) {
+    if (p < kWordMaxP) return 0;
+    for (int l = kNttLogMin; l <= kSmallLogMax; ++l)
+        if (ntt_length_usable(p, 1ull << l)) return 1u << l;
     return 0;
 }
 
@@ -230,6 +312,13 @@ int launch_group(llg_batch* b, Group& g, cudaStream_t caller) {
     const int cnt = (int)g.items.size();
     if (g.n == 0) {
         CK(launch_word((const SmallJob*)g.d_jobs, cnt, (uint64_t*)g.d_results, g.st));
+    } else if (b->engine == LLG_ENGINE_NTT) {
+        const uint64_t* qtw = nullptr;
+        NttConst K;
+        int rc = get_ntt(b->dev, ilog2_exact(g.n), &qtw, &K);
+        if (rc) return rc;
+        CK(launch_small_ntt(ilog2_exact(g.n), (const SmallJob*)g.d_jobs, cnt, qtw, K, (int64_t*)g.d_digits,
+                            (SmallResult*)g.d_results, g.st));
     } else {
         const double2* qtw = nullptr;
         int rc = get_qtw(b->dev, ilog2_exact(g.n) - 1, &qtw);
@@ -401,7 +490,8 @@ int run_large(const Item& item, llg_result& r, std::vector<uint64_t>* words, cud
 // (the reference's batch returns such exponents with seconds < 0, cuda/ll_ntt.cu:259-267).
 int make_batch(const uint64_t* ps, size_t count, uint64_t max_iters, int engine, uint32_t n_force,
                bool strict, int flags, llg_batch** outb) {
-    if (engine != LLG_ENGINE_FP64) return fail(LLG_E_UNSUPPORTED, "engine %d not available", engine);
+    if (engine != LLG_ENGINE_FP64 && engine != LLG_ENGINE_NTT) return fail(LLG_E_ARG, "unknown engine %d", engine);
+    const bool ntt = engine == LLG_ENGINE_NTT;
     int dev;
     int rc = device_ready(&dev);
     if (rc) return rc;
@@ -424,11 +514,11 @@ int make_batch(const uint64_t* ps, size_t count, uint64_t max_iters, int engine,
         Item it{i, p, iters, 0, 0};
         if (p >= kWordMaxP) {
             uint32_t n = n_force;
-            if (n_force && !fp64_length_usable(p, n_force)) {
+            if (n_force && !(ntt ? ntt_length_usable(p, n_force) : fp64_length_usable(p, n_force))) {
                 destroy_batch(b);
                 return fail(LLG_E_UNSUPPORTED, "length %u not usable for p=%llu", n_force, (unsigned long long)p);
             }
-            if (!n) n = fp64_length(p, g_max_bpw);
+            if (!n) n = ntt ? ntt_len(p) : fp64_length(p, g_max_bpw);
             if (!n) {
                 b->out[i].status = LLG_E_UNSUPPORTED;
                 if (strict) {
@@ -614,13 +704,15 @@ int llg_set_max_bpw(double b) {
 
 double llg_get_max_bpw(void) { return g_max_bpw; }
 
-uint32_t llg_ntt_length(uint64_t p) {
-    (void)p;
-    return 0;
-}
+uint32_t llg_ntt_length(uint64_t p) { return ntt_len(p); }
 
 uint64_t llg_max_exponent(int engine) {
     if (engine == LLG_ENGINE_FP64) return (uint64_t)std::floor(g_max_bpw * (double)(1u << kLargeLogMax));
+    if (engine == LLG_ENGINE_NTT) {
+        uint64_t best = 0;
+        for (int l = kSmallLogMin; l <= kSmallLogMax; ++l) best = (uint64_t)((63 - l) / 2) << l;
+        return best;
+    }
     return 0;
 }
 

@@ -30,8 +30,18 @@ cudaError_t launch_small_fp64(int log_n, const SmallJob* jobs, int njobs, const 
                               int64_t* digits, SmallResult* results, float* errlog,
                               double abort_err, cudaStream_t st);
 
-// p < 64: exact 128-bit word arithmetic, one thread per exponent.
+// p < 256: exact multi-limb word arithmetic, one thread per exponent (4 limbs out per exponent).
 cudaError_t launch_word(const SmallJob* jobs, int njobs, uint64_t* res, cudaStream_t st);
+
+// Goldilocks constants of one NTT length N: an N-th root of 2, its inverse, N^-1 (mod q).
+struct NttConst {
+    uint64_t root2, inv_root2, invN;
+};
+
+// Exact NTT whole-test kernel, N = 2^log_n with 5 <= log_n <= 13 (qtw: padded quarter table of the
+// N-point transform, gl::qpad8 layout).
+cudaError_t launch_small_ntt(int log_n, const SmallJob* jobs, int njobs, const uint64_t* qtw, NttConst K,
+                             int64_t* digits, SmallResult* results, cudaStream_t st);
 
 // ---- two-pass engine (N = 2^16 .. 2^23): state resident in HBM ------------------------------
 

@@ -87,3 +87,44 @@ def test_trivial_exponents(gpu):
     assert gpu.run(4)["is_zero"] == 0
     assert gpu.run(1)["is_zero"] == 0
     assert gpu.run(0)["is_zero"] == 0
+
+
+# ---- the exact Goldilocks NTT engine ----------------------------------------------------------
+
+@pytest.mark.parametrize("logn", range(6, 14))
+def test_ntt_every_length_full_residue(gpu, oracle, logn):
+    """Every NTT length at bits per digit spanning the exactness bound ceil(p/N) <= (63-log2 N)/2."""
+    n = 1 << logn
+    hi = ((63 - logn) // 2) * n
+    lo = max(256, n * ((logn + 12 + 3) // 4))
+    rng = random.Random(100 + logn)
+    ps = [p for p in oracle.primes(lo, min(hi, 40000)) if p % 2]
+    picks = rng.sample(ps, min(3, len(ps))) + ([max(ps)] if ps else [])
+    for p in picks:
+        r = gpu.run(p, engine="ntt", n=n, want_words=True)
+        assert r["status"] == 0 and r["n"] == n
+        assert r["words"] == oracle.ll_gmp(p)[2], (p, n)
+
+
+def test_ntt_length_rule_matches_reference():
+    from mersenneprime_python_cpp_gmp_benchmark_b200 import llgpu
+    from oracle import oracle
+    # the reference's ntt_length (cuda/ll_ntt.cu:176-180), where its own kernel can run (p >= 256)
+    for p in (521, 1279, 4423, 9689, 44497, 100003, 204799):
+        assert llgpu.ntt_length(p) == oracle.lib().orc_ntt_length(p), p
+
+
+def test_ntt_matches_fp64_and_oracle_batch(gpu, oracle):
+    ps = [p for p in oracle.primes(320, 12000)][::5]  # the NTT takes p >= 5 * 64 (bits-per-digit floor)
+    a = gpu.run_batch(ps, engine="ntt", want_words=True)
+    b = gpu.run_batch(ps, engine="fp64", want_words=True)
+    for p, ra, rb in zip(ps, a, b):
+        assert ra["status"] == 0 and ra["words"] == rb["words"], p
+    for p, ra in list(zip(ps, a))[::10]:
+        assert ra["words"] == oracle.ll_gmp(p)[2], p
+
+
+def test_ntt_interim_residue(gpu, oracle):
+    for p, k in ((4423, 3), (86243, 1000), (204791, 77)):
+        r = gpu.run(p, iters=k, engine="ntt", want_words=True)
+        assert r["words"] == oracle.ll_gmp(p, k)[2]

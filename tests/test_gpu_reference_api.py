@@ -53,6 +53,13 @@ def test_cuda_engine(ll, lc, oracle):
     assert sms > 0 and mem > 0 and lc.max_exponent() > 0
 
 
+def test_cuda_engine_ntt(ll, lc, oracle):
+    """lucaslehmer_cuda's own engine (cuda/ll_ntt.cu) is the exact NTT: the same contract."""
+    res = {p: r for p, r, s, res64 in lc.lucas_lehmer_batch(ll.primes(2, 4423), engine="ntt") if s >= 0}
+    assert sorted(p for p, r in res.items() if r) == [p for p in KNOWN if p in res]
+    assert all(res[p] == oracle.ll_gmp(p)[0] for p in res)
+
+
 def test_res64_agrees_across_engines(ll):
     # reference tests/test_lucaslehmer.py:49-53, against the reference's own values
     gold = {row["p"]: (row["is_prime"], int(row["res64"], 16)) for row in load_json("appendix.json")["full"]}
