@@ -108,16 +108,17 @@ int llg_batch_errlog(llg_batch* b, float* log, size_t cap, size_t* len);
 int llg_batch_device_ms(llg_batch* b, float* ms);
 void llg_batch_destroy(llg_batch* b);
 
-/* One exponent's device state on the two-pass engine (lengths 2^14 .. 2^23), for callers that
+/* One exponent's device state on a two-pass engine (FP64 or NTT, lengths 2^14 .. 2^23), for callers that
  * drive the iterations themselves (interim residues, timing on their own stream):
  * create (tables, state; n == 0 picks the length), start (s_0 = 4 and the first squaring),
  * iterate (enqueue squarings as CUDA-graph replays, no host sync), read (final row pass, digits
- * back, exact residue; waits). llg_result.iters counts the squarings done since start;
+ * back, exact residue; waits; the squarings may resume after it). llg_result.iters counts the
+ * squarings done since s_0 (start's included);
  * llg_result.status is LLG_E_ROUNDOFF when the worst round-off exceeded 0.4 (no escalation here).
- * llg_test_errlog: per-squaring max round-off (ring of 65536 entries).
+ * llg_test_errlog (FP64): per-squaring max round-off (ring of 65536 entries).
  * Replaces the iteration loop of lucas_lehmer_fft_raw(), lucaslehmer.cpp:281-311, for large p. */
 typedef struct llg_test llg_test;
-int llg_test_create(uint64_t p, uint32_t n, llg_test** out);
+int llg_test_create(uint64_t p, uint32_t n, int engine, llg_test** out);
 int llg_test_start(llg_test* t, void* stream);
 int llg_test_iterate(llg_test* t, uint64_t iters, void* stream);
 int llg_test_read(llg_test* t, void* stream, llg_result* out, uint64_t* words, size_t nwords);

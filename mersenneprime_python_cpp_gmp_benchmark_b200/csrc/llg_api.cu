@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -197,13 +198,13 @@ constexpr int kNttLogMin = 6;  // N = 64, the reference's shortest NTT (cuda/ll_
 
 bool ntt_length_usable(uint64_t p, uint64_t n) {
     const int l = ilog2_exact(n);
-    if (l < kNttLogMin || l > kSmallLogMax) return false;
+    if (l < kNttLogMin || (l > kSmallLogMax && !ntt_large_length_supported(l))) return false;
     return (p + n - 1) / n <= (uint64_t)((63 - l) / 2) && 4 * (p / n) >= (uint64_t)l + 12;
 }
 
 uint32_t ntt_len(uint64_t p) {
     if (p < kWordMaxP) return 0;
-    for (int l = kNttLogMin; l <= kSmallLogMax; ++l)
+    for (int l = kNttLogMin; l <= kLargeLogMax; ++l)
         if (ntt_length_usable(p, 1ull << l)) return 1u << l;
     return 0;
 }
@@ -407,14 +408,15 @@ double bits_to_double(unsigned long long b) {
     return d;
 }
 
-int run_large(const Item& item, llg_result& r, std::vector<uint64_t>* words, cudaStream_t st) {
+template <class TestT>
+int run_large_t(const Item& item, llg_result& r, std::vector<uint64_t>* words, cudaStream_t st) {
     uint32_t n = item.n;
     uint32_t esc = item.escalations;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     for (;;) {
-        LargeTest T;
+        TestT T;
         CK(T.init(item.p, ilog2_exact(n)));
         CK(cudaEventRecord(e0, st));
         CK(T.start(seed_digits(n), st));
@@ -450,7 +452,7 @@ int run_large(const Item& item, llg_result& r, std::vector<uint64_t>* words, cud
             if (worst > kAbortErrLarge) abort = true;
         }
         r.max_err = std::max(r.max_err, worst);
-        if (abort) {
+        if (abort) {  // FP64 only: the NTT's round-off is identically zero
             const uint32_t nn = next_fp64_length(item.p, n);
             if (!nn) {
                 r.status = LLG_E_ROUNDOFF;
@@ -483,6 +485,11 @@ int run_large(const Item& item, llg_result& r, std::vector<uint64_t>* words, cud
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     return LLG_OK;
+}
+
+int run_large(int engine, const Item& item, llg_result& r, std::vector<uint64_t>* words, cudaStream_t st) {
+    return engine == LLG_ENGINE_NTT ? run_large_t<NttLargeTest>(item, r, words, st)
+                                    : run_large_t<LargeTest>(item, r, words, st);
 }
 
 // Creates a batch: trivial exponents resolved on the host, the rest grouped by length.
@@ -620,7 +627,7 @@ int collect_batch(llg_batch* b) {
             st = own;
         }
         for (const Item& it : large) {
-            const int rc = run_large(it, b->out[it.idx], b->keep_words ? &b->words[it.idx] : nullptr, st);
+            const int rc = run_large(b->engine, it, b->out[it.idx], b->keep_words ? &b->words[it.idx] : nullptr, st);
             if (rc) {
                 if (own) cudaStreamDestroy(own);
                 return rc;
@@ -708,11 +715,7 @@ uint32_t llg_ntt_length(uint64_t p) { return ntt_len(p); }
 
 uint64_t llg_max_exponent(int engine) {
     if (engine == LLG_ENGINE_FP64) return (uint64_t)std::floor(g_max_bpw * (double)(1u << kLargeLogMax));
-    if (engine == LLG_ENGINE_NTT) {
-        uint64_t best = 0;
-        for (int l = kSmallLogMin; l <= kSmallLogMax; ++l) best = (uint64_t)((63 - l) / 2) << l;
-        return best;
-    }
+    if (engine == LLG_ENGINE_NTT) return (uint64_t)((63 - kLargeLogMax) / 2) << kLargeLogMax;
     return 0;
 }
 
@@ -803,27 +806,42 @@ void llg_batch_destroy(llg_batch* b) { destroy_batch(b); }
 }  // extern "C"
 
 struct llg_test {
-    llg::LargeTest T;
+    std::unique_ptr<llg::LargeTest> f;     // FP64 engine
+    std::unique_ptr<llg::NttLargeTest> n;  // NTT engine
     int dev = -1;
+    uint64_t p() const { return f ? f->p : n->p; }
+    int logN() const { return f ? f->logN : n->logN; }
+    uint64_t done() const { return f ? f->done : n->done; }
 };
 
 extern "C" {
 
-int llg_test_create(uint64_t p, uint32_t n, llg_test** out) {
+int llg_test_create(uint64_t p, uint32_t n, int engine, llg_test** out) {
     if (!out) return fail(LLG_E_ARG, "null pointer");
     *out = nullptr;
+    if (engine != LLG_ENGINE_FP64 && engine != LLG_ENGINE_NTT) return fail(LLG_E_ARG, "unknown engine %d", engine);
     int dev;
     int rc = device_ready(&dev);
     if (rc) return rc;
     if (p < 3 || p % 2 == 0) return fail(LLG_E_ARG, "p must be odd and >= 3");
-    if (n == 0) n = fp64_length(p, g_max_bpw);
+    const bool ntt = engine == LLG_ENGINE_NTT;
+    if (n == 0) n = ntt ? ntt_len(p) : fp64_length(p, g_max_bpw);
     const int l = ilog2_exact(n);
-    if (l <= kSmallLogMax || !large_length_supported(l) || !fp64_length_usable(p, n))
-        return fail(LLG_E_UNSUPPORTED, "length %u not usable by the two-pass engine for p=%llu", n,
-                    (unsigned long long)p);
+    const bool ok = ntt ? (l > kSmallLogMax && ntt_large_length_supported(l) && ntt_length_usable(p, n))
+                        : (l > kSmallLogMax && large_length_supported(l) && fp64_length_usable(p, n));
+    if (!ok)
+        return fail(LLG_E_UNSUPPORTED, "length %u not usable by the two-pass %s engine for p=%llu", n,
+                    ntt ? "NTT" : "FP64", (unsigned long long)p);
     llg_test* t = new llg_test();
     t->dev = dev;
-    cudaError_t e = t->T.init(p, l);
+    cudaError_t e;
+    if (ntt) {
+        t->n.reset(new llg::NttLargeTest());
+        e = t->n->init(p, l);
+    } else {
+        t->f.reset(new llg::LargeTest());
+        e = t->f->init(p, l);
+    }
     if (e != cudaSuccess) {
         delete t;
         return fail(e == cudaErrorMemoryAllocation ? LLG_E_NOMEM : LLG_E_CUDA, "CUDA: %s", cudaGetErrorString(e));
@@ -835,31 +853,39 @@ int llg_test_create(uint64_t p, uint32_t n, llg_test** out) {
 int llg_test_start(llg_test* t, void* stream) {
     if (!t) return fail(LLG_E_ARG, "null test");
     cudaStream_t st = stream ? (cudaStream_t)stream : default_stream_for_thread();
-    CK(t->T.start(seed_digits(1ull << t->T.logN), st));
+    const std::vector<int> seed = seed_digits(1ull << t->logN());
+    if (t->f) CK(t->f->start(seed, st));
+    else CK(t->n->start(seed, st));
     return LLG_OK;
 }
 
 int llg_test_iterate(llg_test* t, uint64_t iters, void* stream) {
     if (!t) return fail(LLG_E_ARG, "null test");
     cudaStream_t st = stream ? (cudaStream_t)stream : default_stream_for_thread();
-    CK(t->T.step(iters, st));
+    if (t->f) CK(t->f->step(iters, st));
+    else CK(t->n->step(iters, st));
     return LLG_OK;
 }
 
 int llg_test_read(llg_test* t, void* stream, llg_result* out, uint64_t* words, size_t nwords) {
     if (!t || !out) return fail(LLG_E_ARG, "null pointer");
-    const uint64_t p = t->T.p;
+    const uint64_t p = t->p();
     const size_t nw = (size_t)((p + 63) / 64);
     if (words && nwords < nw) return fail(LLG_E_ARG, "words buffer too small");
     cudaStream_t st = stream ? (cudaStream_t)stream : default_stream_for_thread();
     std::vector<int> digits;
-    CK(t->T.finish(st, digits));
     LargeCtl h;
-    CK(t->T.read_ctl(h, st));
+    if (t->f) {
+        CK(t->f->finish(st, digits));
+        CK(t->f->read_ctl(h, st));
+    } else {
+        CK(t->n->finish(st, digits));
+        CK(t->n->read_ctl(h, st));
+    }
     std::memset(out, 0, sizeof *out);
     out->p = p;
-    out->iters = t->T.done;
-    out->n = 1u << t->T.logN;
+    out->iters = t->done();
+    out->n = 1u << t->logN();
     out->max_err = bits_to_double(h.err_max);
     if (h.timeout) return fail(LLG_E_TIMEOUT, "carry wait timed out");
     std::vector<int64_t> d64(digits.begin(), digits.end());
@@ -873,9 +899,10 @@ int llg_test_read(llg_test* t, void* stream, llg_result* out, uint64_t* words, s
 
 int llg_test_errlog(llg_test* t, float* log, size_t cap, size_t* len) {
     if (!t || !log) return fail(LLG_E_ARG, "null pointer");
-    const size_t have = (size_t)std::min<uint64_t>(t->T.done, (uint64_t)t->T.errlog_len);
+    if (!t->f) return fail(LLG_E_ARG, "the NTT engine has no round-off log (it is exact)");
+    const size_t have = (size_t)std::min<uint64_t>(t->f->done, (uint64_t)t->f->errlog_len);
     const size_t n = std::min(cap, have);
-    CK(cudaMemcpy(log, t->T.errlog, n * sizeof(float), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(log, t->f->errlog, n * sizeof(float), cudaMemcpyDeviceToHost));
     if (len) *len = n;
     return LLG_OK;
 }

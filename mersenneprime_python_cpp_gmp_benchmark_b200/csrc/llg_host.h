@@ -49,4 +49,28 @@ struct LargeTest {
     cudaError_t clear_err_since(cudaStream_t st);
 };
 
+// Device state of one exponent on the two-pass NTT engine (same launch sequence as LargeTest).
+struct NttLargeTest {
+    uint64_t p = 0, N = 0;
+    int logN = 0, logC = 0, logR = 0, C = 0, R = 0, nblocks = 0;
+    void* mem[20] = {};
+    int nmem = 0;
+    NttLargeArgs args{};
+    cudaGraphExec_t exec = nullptr;
+    uint64_t done = 0;
+    LargeCtl* ctl = nullptr;
+    int* digits = nullptr;
+
+    ~NttLargeTest();
+    cudaError_t init(uint64_t p, int log_n);
+    cudaError_t start(const std::vector<int>& digits, cudaStream_t st);
+    cudaError_t step(uint64_t k, cudaStream_t st);
+    cudaError_t finish(cudaStream_t st, std::vector<int>& out);
+    cudaError_t read_ctl(LargeCtl& h, cudaStream_t st);
+};
+
+bool ntt_large_length_supported(int log_n);
+// exact N-th root of 2, its inverse, w_N and N^-1 in GF(q) (host arithmetic)
+bool ntt_host_constants(int log_n, uint64_t& omega, uint64_t& root2, uint64_t& inv_root2, uint64_t& invN);
+
 }  // namespace llg

@@ -55,10 +55,29 @@ struct LargeCtl {
     unsigned int timeout;            // set when a bounded wait gave up (the result is then invalid)
     unsigned long long err_max;      // bits of the max round-off over the run (double, >= 0)
     unsigned long long err_since;    // same, since the host last cleared it
+    unsigned int halo_read;          // epoch + 1 once block 0 has read the wrap-around rows
     unsigned int flags[kLargeMaxBlocks];  // flags[k] = epoch + 1 once block k published its carries
 };
 
 enum { LARGE_INIT = 0, LARGE_ITER = 1, LARGE_FINAL = 2 };
+
+#ifdef __CUDACC__
+// Bounded wait until *f >= target. On giving up it sets ctl->timeout (the run's result is then
+// reported invalid) and returns, so a kernel never spins forever.
+__device__ __forceinline__ void wait_flag(unsigned int* f, unsigned int target, LargeCtl* ctl,
+                                          unsigned long long limit) {
+    volatile unsigned int* vf = f;
+    unsigned long long spins = 0;
+    while (*vf < target) {
+        if (++spins > limit) {
+            atomicExch(&ctl->timeout, 1u);
+            break;
+        }
+        __nanosleep(64);
+    }
+    __threadfence();
+}
+#endif
 
 struct LargeArgs {
     double2* V;               // state: element (row a, column slot pos) at pos * R + a
@@ -88,5 +107,37 @@ struct LargeArgs {
 
 cudaError_t launch_large_row(int log_c, int mode, const LargeArgs& a, cudaStream_t st);
 cudaError_t launch_large_col(int log_r, const LargeArgs& a, cudaStream_t st);
+
+// ---- two-pass exact NTT engine (N = 2^14 .. 2^23): N field elements in HBM ------------------
+
+struct NttLargeArgs {
+    uint64_t* V;              // state: element (row a, column slot pos) at pos * R + a
+    const uint64_t* qtwC;     // padded quarter table of the C-point row NTT (gl::qpad8)
+    const uint64_t* qtwR;     // padded quarter table of the R-point column NTT
+    const uint64_t* tw1;      // w_N^x, x < 2^tw_shift
+    const uint64_t* tw2;      // w_N^(y 2^tw_shift)
+    const int* pos_of_c;      // column slot of row-NTT frequency c
+    const uint64_t* wA;       // [R] w^sA(a), w an N-th root of 2
+    const uint64_t* iwA;      // [R] w^-sA(a)
+    const int* sA;            // [R] (-a p) mod N
+    const uint64_t* wB;       // [C] w^sB(b)
+    const uint64_t* iwB;      // [C] w^-sB(b) / N
+    const int* sB;            // [C] (-R b p) mod N
+    long long* c1;            // [nblocks][C] hop-1 carry-outs of each block's last row
+    int* c2;                  // [nblocks][C] hop-2 carry-outs
+    int* c3;                  // [nblocks][C] hop-3 carry-outs
+    long long* halo;          // block 0's wrap-around carries: C int64 + 2 * C int32
+    LargeCtl* ctl;
+    int* digits;              // N int32, natural order (INIT input; dump / FINAL output)
+    int dump;
+    int tw_shift;
+    int C, R, nblocks;
+    int q, rem;
+    int logN;
+};
+
+cudaError_t launch_ntt_row(int log_c, int mode, const NttLargeArgs& a, cudaStream_t st);
+cudaError_t launch_ntt_col(int log_r, const NttLargeArgs& a, cudaStream_t st);
+cudaError_t configure_ntt_large(int log_c, int log_r);
 
 }  // namespace llg

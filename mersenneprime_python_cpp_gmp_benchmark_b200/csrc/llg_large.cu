@@ -86,7 +86,11 @@ __global__ void __launch_bounds__(kRowG * (1 << LOG_C) / (1 << kLargeLogE), 2) l
             s_blk = blockIdx.x;
         } else {
             const int b = (int)atomicAdd(&A.ctl->ticket[ep & 1], 1u);
-            if (b == A.nblocks - 1) A.ctl->ticket[(ep + 1) & 1] = 0u;
+            if (b == A.nblocks - 1) {
+                // every block of this launch holds its ticket: both counters can be reset
+                A.ctl->ticket[(ep + 1) & 1] = 0u;
+                A.ctl->ticket[ep & 1] = 0u;
+            }
             s_blk = b;
         }
         s_err = 0ull;
@@ -115,50 +119,60 @@ __global__ void __launch_bounds__(kRowG * (1 << LOG_C) / (1 << kLargeLogE), 2) l
             x1s[i] = d.y;
         }
     } else {
-        // ---- wrap-around carries into row 0 (2^p == 1): block 0 recomputes rows R-2 and R-1
-        //      (every row group runs the same computation so the FFT's barriers stay uniform).
+        // ---- wrap-around carries into row 0 (2^p == 1): block 0 recomputes rows R-2 (row group 0)
+        //      and R-1 (the other row groups, which keeps the FFT's barriers uniform) side by side.
         //      Row R-1, column b feeds row 0, column b+1; column C-1 wraps to digit 0. ----
         if (blk == 0) {
-#pragma unroll 1
-            for (int hrow = 0; hrow < 2; ++hrow) {
-                const int ah = R - 2 + hrow;
+            const int ah = R - 2 + (rg > 0 ? 1 : 0);
 #pragma unroll
-                for (int j = 0; j < E; ++j) {
-                        v[j] = A.V[(size_t)(tr * E + j) * R + ah];
-                }
-                inverse_from<GC, GC::P - 1, false>(v, buf, qtw, tr, gsync);
-                const int h0 = __ldg(A.sA + 2 * ah), h1 = __ldg(A.sA + 2 * ah + 1);
-                const double ih0 = __ldg(A.iwA + 2 * ah), ih1 = __ldg(A.iwA + 2 * ah + 1);
+            for (int j = 0; j < E; ++j) v[j] = A.V[(size_t)(tr * E + j) * R + ah];
+            inverse_from<GC, GC::P - 1, false>(v, buf, qtw, tr, gsync);
+            __syncthreads();
+            if (t == 0) {
+                // rows R-2 and R-1 are read: the last block may overwrite them
+                __threadfence();
+                *reinterpret_cast<volatile unsigned*>(&A.ctl->halo_read) = ep + 1u;
+            }
+            const int h0 = __ldg(A.sA + 2 * ah), h1 = __ldg(A.sA + 2 * ah + 1);
+            const double ih0 = __ldg(A.iwA + 2 * ah), ih1 = __ldg(A.iwA + 2 * ah + 1);
+            long long hc[E];
+#pragma unroll
+            for (int i = 0; i < E; ++i) {
+                const int b = tr + TR * i;
+                const int sb = __ldg(A.sB + b);
+                const double iwb = __ldg(A.iwB + b);
+                const bool o0 = h0 + sb >= N, o1 = h1 + sb >= N;
+                const int s0 = o0 ? h0 + sb - N : h0 + sb, s1 = o1 ? h1 + sb - N : h1 + sb;
+                const int b0 = A.q + (s0 < A.rem), b1 = A.q + (s1 < A.rem);
+                const double va = v[i].x * (ih0 * iwb) * (o0 ? 2.0 : 1.0);
+                const double vb = v[i].y * (ih1 * iwb) * (o1 ? 2.0 : 1.0);
+                long long la, lb, c;
+                const double ra = round_shift(va, la), rb = round_shift(vb, lb);
+                lerr = fmax(lerr, fmax(fabs(va - ra), fabs(vb - rb)));
+                x0s[i] = (int)balance(la, b0, c);
+                x1s[i] = (int)balance(lb + c, b1, c);
+                hc[i] = c;
+                if (rg == 0) hc1[b] = c;
+            }
+            __syncthreads();
+            if (rg == 1) {
+                // second hop of row R-1 with row R-2's carry-out (same column)
 #pragma unroll
                 for (int i = 0; i < E; ++i) {
                     const int b = tr + TR * i;
                     const int sb = __ldg(A.sB + b);
-                    const double iwb = __ldg(A.iwB + b);
                     const bool o0 = h0 + sb >= N, o1 = h1 + sb >= N;
                     const int s0 = o0 ? h0 + sb - N : h0 + sb, s1 = o1 ? h1 + sb - N : h1 + sb;
                     const int b0 = A.q + (s0 < A.rem), b1 = A.q + (s1 < A.rem);
-                    const double va = v[i].x * (ih0 * iwb) * (o0 ? 2.0 : 1.0);
-                    const double vb = v[i].y * (ih1 * iwb) * (o1 ? 2.0 : 1.0);
-                    long long la, lb, c;
-                    const double ra = round_shift(va, la), rb = round_shift(vb, lb);
-                    lerr = fmax(lerr, fmax(fabs(va - ra), fabs(vb - rb)));
-                    long long x0 = balance(la, b0, c);
-                    long long x1 = balance(lb + c, b1, c);
-                    const long long cout = c;
-                    if (hrow == 0) {
-                        if (rg == 0) hc1[b] = cout;
-                    } else {
-                        // second hop of row R-1 with row R-2's carry-out (same column)
-                        x0 = balance(x0 + hc1[b], b0, c);
-                        balance(x1 + c, b1, c);
-                        if (rg == 0) {
-                            hin[(b + 1) & (C - 1)] = cout;
-                            hin2[(b + 1) & (C - 1)] = (int)c;
-                        }
-                    }
+                    long long c;
+                    const long long x0 = balance((long long)x0s[i] + hc1[b], b0, c);
+                    balance((long long)x1s[i] + c, b1, c);
+                    (void)x0;
+                    hin[(b + 1) & (C - 1)] = hc[i];
+                    hin2[(b + 1) & (C - 1)] = (int)c;
                 }
-                __syncthreads();
             }
+            __syncthreads();
         }
 
         // ---- load the block's rows (coalesced: kRowG contiguous values per column slot) ----
@@ -228,19 +242,7 @@ __global__ void __launch_bounds__(kRowG * (1 << LOG_C) / (1 << kLargeLogE), 2) l
         if (t == 0) {
             __threadfence();
             *reinterpret_cast<volatile unsigned*>(&A.ctl->flags[blk]) = ep + 1u;
-            if (blk > 0) {
-                // wait (bounded) for block blk-1's carry-outs
-                volatile unsigned* f = &A.ctl->flags[blk - 1];
-                unsigned long long spins = 0;
-                while (*f < ep + 1u) {
-                    if (++spins > kSpinLimit) {
-                        atomicExch(&A.ctl->timeout, 1u);
-                        break;
-                    }
-                    __nanosleep(64);
-                }
-                __threadfence();
-            }
+            if (blk > 0) wait_flag(&A.ctl->flags[blk - 1], ep + 1u, A.ctl, kSpinLimit);  // block blk-1's carries
         }
         __syncthreads();
         // hop 2 for the block's first row: previous block's last row, or the wrap
@@ -306,6 +308,10 @@ __global__ void __launch_bounds__(kRowG * (1 << LOG_C) / (1 << kLargeLogE), 2) l
     forward_from<GC, 0>(v, buf, qtw, tr, gsync);
 #pragma unroll
     for (int j = 0; j < E; ++j) buf[phys(tr * E + j)] = v[j];
+    if (MODE == LARGE_ITER && blk == A.nblocks - 1 && t == 0) {
+        // rows R-2 and R-1 are block 0's wrap-around input: wait (bounded) until it has read them
+        wait_flag(&A.ctl->halo_read, ep + 1u, A.ctl, kSpinLimit);
+    }
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < G * C / T; ++r) {

@@ -227,6 +227,8 @@ cudaError_t LargeTest::step(uint64_t k, cudaStream_t st) {
 cudaError_t LargeTest::finish(cudaStream_t st, std::vector<int>& out) {
     cudaError_t e;
     if ((e = launch_large_row(logC, LARGE_FINAL, args, st))) return e;
+    // the squarings may resume from this state at the same epoch: clear the flags FINAL set
+    if ((e = cudaMemsetAsync(&ctl->halo_read, 0, sizeof(LargeCtl) - offsetof(LargeCtl, halo_read), st))) return e;
     out.resize(2 * M);
     if ((e = cudaMemcpyAsync(out.data(), digits, 2 * M * sizeof(int), cudaMemcpyDeviceToHost, st))) return e;
     return cudaStreamSynchronize(st);
@@ -247,6 +249,239 @@ std::vector<int> seed_digits(uint64_t n) {
     std::vector<int> d(n, 0);
     d[0] = 4;
     return d;
+}
+
+}  // namespace llg
+
+// ---- two-pass NTT engine ----------------------------------------------------------------------
+
+namespace llg {
+
+namespace {
+
+constexpr uint64_t kQ = 0xFFFFFFFF00000001ull;
+uint64_t qmul(uint64_t a, uint64_t b) { return (uint64_t)(((unsigned __int128)a * b) % kQ); }
+uint64_t qpow(uint64_t a, uint64_t e) {
+    uint64_t r = 1;
+    a %= kQ;
+    while (e) {
+        if (e & 1) r = qmul(r, a);
+        a = qmul(a, a);
+        e >>= 1;
+    }
+    return r;
+}
+
+int ntt_pos_of_freq(int log_l, int k) {  // SmallGeom<log_l> (16 values per thread) digit reversal
+    const int L = 1 << log_l, P = (log_l + 3) / 4;
+    const int RLAST = (log_l % 4 == 0) ? 16 : (1 << (log_l % 4));
+    const int klast = k / (L / RLAST);
+    int low = k % (L / RLAST), rest = 0;
+    for (int q = 0; q < P - 1; ++q) {
+        rest = (rest << 4) | (low & 15);
+        low >>= 4;
+    }
+    return rest * RLAST + klast;
+}
+
+std::vector<uint64_t> ntt_quarter(int log_l) {  // w_L^r at gl::qpad8(r), r < L/4
+    const uint32_t L = 1u << log_l, QL = L / 4;
+    std::vector<uint64_t> t(QL + (QL >> 4) + 1, 0ull);
+    const uint64_t w = qpow(7, (kQ - 1) / L);
+    uint64_t x = 1;
+    for (uint32_t r = 0; r < QL; ++r) {
+        t[r + (r >> 4)] = x;
+        x = qmul(x, w);
+    }
+    return t;
+}
+
+}  // namespace
+
+bool ntt_host_constants(int log_n, uint64_t& omega, uint64_t& root2, uint64_t& inv_root2, uint64_t& invN) {
+    // cuda/ll_ntt.cu:182-195: w_N = 7^((q-1)/N); an N-th root of 2 from a primitive (192N)-th root
+    const uint64_t N = 1ull << log_n;
+    omega = qpow(7, (kQ - 1) / N);
+    const uint64_t om = qpow(7, (kQ - 1) / (192 * N)), r192 = qpow(om, N);
+    uint64_t pw = 1, s = 0;
+    for (; s < 192; ++s) {
+        if (pw == 2) break;
+        pw = qmul(pw, r192);
+    }
+    if (s == 192) return false;
+    root2 = qpow(om, s);
+    inv_root2 = qpow(root2, kQ - 2);
+    invN = qpow(N % kQ, kQ - 2);
+    return true;
+}
+
+bool ntt_large_length_supported(int log_n) { return log_n >= 14 && log_n <= 23; }
+
+NttLargeTest::~NttLargeTest() {
+    if (exec) cudaGraphExecDestroy(exec);
+    for (int i = 0; i < nmem; ++i)
+        if (mem[i]) cudaFree(mem[i]);
+}
+
+cudaError_t NttLargeTest::init(uint64_t p_, int log_n) {
+    p = p_;
+    logN = log_n;
+    N = 1ull << logN;
+    logC = std::min(10, std::max(7, logN / 2));
+    logR = logN - logC;
+    C = 1 << logC;
+    R = 1 << logR;
+    nblocks = R / 4;
+    const int s = std::max(logC, (logN + 1) / 2);
+    cudaError_t e;
+    if ((e = configure_ntt_large(logC, logR))) return e;
+    uint64_t omega, root2, iroot2, invN;
+    if (!ntt_host_constants(logN, omega, root2, iroot2, invN)) return cudaErrorInvalidValue;
+    auto up = [&](const auto& vec, const auto** dptr) -> cudaError_t {
+        const size_t bytes = vec.size() * sizeof(vec[0]);
+        void* d = nullptr;
+        cudaError_t er = cudaMalloc(&d, bytes);
+        if (er) return er;
+        mem[nmem++] = d;
+        *dptr = static_cast<decltype(vec.data())>(d);
+        return cudaMemcpy(d, vec.data(), bytes, cudaMemcpyHostToDevice);
+    };
+    auto alloc = [&](size_t bytes, void** d) -> cudaError_t {
+        cudaError_t er = cudaMalloc(d, bytes);
+        if (!er) mem[nmem++] = *d;
+        return er;
+    };
+    NttLargeArgs& A = args;
+    std::memset(&A, 0, sizeof A);
+    std::vector<uint64_t> qc = ntt_quarter(logC), qr = ntt_quarter(logR);
+    std::vector<uint64_t> t1(1ull << s), t2(N >> s);
+    {
+        uint64_t x = 1;
+        for (size_t i = 0; i < t1.size(); ++i) {
+            t1[i] = x;
+            x = qmul(x, omega);
+        }
+        const uint64_t st = qpow(omega, 1ull << s);
+        x = 1;
+        for (size_t i = 0; i < t2.size(); ++i) {
+            t2[i] = x;
+            x = qmul(x, st);
+        }
+    }
+    std::vector<int> pc(C), hsA(R), hsB(C);
+    for (int c = 0; c < C; ++c) pc[c] = ntt_pos_of_freq(logC, c);
+    std::vector<uint64_t> hwA(R), hiwA(R), hwB(C), hiwB(C);
+    for (int a = 0; a < R; ++a) {
+        const uint64_t sj = (N - (uint64_t)(((unsigned __int128)a * p) % N)) % N;
+        hsA[a] = (int)sj;
+        hwA[a] = qpow(root2, sj);
+        hiwA[a] = qpow(iroot2, sj);
+    }
+    for (int b = 0; b < C; ++b) {
+        const uint64_t sj = (N - (uint64_t)(((unsigned __int128)R * b * p) % N)) % N;
+        hsB[b] = (int)sj;
+        hwB[b] = qpow(root2, sj);
+        hiwB[b] = qmul(qpow(iroot2, sj), invN);
+    }
+    const uint64_t *cqc, *cqr, *ct1, *ct2, *cwA, *ciwA, *cwB, *ciwB;
+    const int *cpc, *csA, *csB;
+    if ((e = up(qc, &cqc)) || (e = up(qr, &cqr)) || (e = up(t1, &ct1)) || (e = up(t2, &ct2)) ||
+        (e = up(pc, &cpc)) || (e = up(hwA, &cwA)) || (e = up(hiwA, &ciwA)) || (e = up(hsA, &csA)) ||
+        (e = up(hwB, &cwB)) || (e = up(hiwB, &ciwB)) || (e = up(hsB, &csB)))
+        return e;
+    void *dV, *dc1, *dc2, *dc3, *dh, *dctl, *dd;
+    if ((e = alloc(N * sizeof(uint64_t), &dV)) || (e = alloc((size_t)nblocks * C * sizeof(long long), &dc1)) ||
+        (e = alloc((size_t)nblocks * C * sizeof(int), &dc2)) || (e = alloc((size_t)nblocks * C * sizeof(int), &dc3)) ||
+        (e = alloc((size_t)C * (sizeof(long long) + 2 * sizeof(int)), &dh)) ||
+        (e = alloc(sizeof(LargeCtl), &dctl)) || (e = alloc(N * sizeof(int), &dd)))
+        return e;
+    if ((e = cudaMemset(dctl, 0, sizeof(LargeCtl)))) return e;
+    ctl = static_cast<LargeCtl*>(dctl);
+    digits = static_cast<int*>(dd);
+    A.V = static_cast<uint64_t*>(dV);
+    A.qtwC = cqc;
+    A.qtwR = cqr;
+    A.tw1 = ct1;
+    A.tw2 = ct2;
+    A.pos_of_c = cpc;
+    A.wA = cwA;
+    A.iwA = ciwA;
+    A.sA = csA;
+    A.wB = cwB;
+    A.iwB = ciwB;
+    A.sB = csB;
+    A.c1 = static_cast<long long*>(dc1);
+    A.c2 = static_cast<int*>(dc2);
+    A.c3 = static_cast<int*>(dc3);
+    A.halo = static_cast<long long*>(dh);
+    A.ctl = ctl;
+    A.digits = digits;
+    A.dump = 0;
+    A.tw_shift = s;
+    A.C = C;
+    A.R = R;
+    A.nblocks = nblocks;
+    A.q = (int)(p >> logN);
+    A.rem = (int)(p & (N - 1));
+    A.logN = logN;
+    return cudaSuccess;
+}
+
+cudaError_t NttLargeTest::start(const std::vector<int>& d, cudaStream_t st) {
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(digits, d.data(), d.size() * sizeof(int), cudaMemcpyHostToDevice, st))) return e;
+    if ((e = cudaMemsetAsync(ctl, 0, sizeof(LargeCtl), st))) return e;
+    if ((e = launch_ntt_row(logC, LARGE_INIT, args, st))) return e;
+    if ((e = launch_ntt_col(logR, args, st))) return e;
+    done = 1;
+    return cudaSuccess;
+}
+
+cudaError_t NttLargeTest::step(uint64_t k, cudaStream_t st) {
+    cudaError_t e;
+    if (!exec && k >= (uint64_t)kGraphChunk) {
+        cudaStream_t cap;
+        if ((e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking))) return e;
+        if ((e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal))) return e;
+        for (int i = 0; i < kGraphChunk; ++i) {
+            launch_ntt_row(logC, LARGE_ITER, args, cap);
+            launch_ntt_col(logR, args, cap);
+        }
+        cudaGraph_t g;
+        e = cudaStreamEndCapture(cap, &g);
+        cudaStreamDestroy(cap);
+        if (e) return e;
+        e = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e) return e;
+    }
+    uint64_t left = k;
+    while (exec && left >= (uint64_t)kGraphChunk) {
+        if ((e = cudaGraphLaunch(exec, st))) return e;
+        left -= kGraphChunk;
+        done += kGraphChunk;
+    }
+    for (uint64_t i = 0; i < left; ++i) {
+        if ((e = launch_ntt_row(logC, LARGE_ITER, args, st))) return e;
+        if ((e = launch_ntt_col(logR, args, st))) return e;
+    }
+    done += left;
+    return cudaSuccess;
+}
+
+cudaError_t NttLargeTest::finish(cudaStream_t st, std::vector<int>& out) {
+    cudaError_t e;
+    if ((e = launch_ntt_row(logC, LARGE_FINAL, args, st))) return e;
+    if ((e = cudaMemsetAsync(&ctl->halo_read, 0, sizeof(LargeCtl) - offsetof(LargeCtl, halo_read), st))) return e;
+    out.resize(N);
+    if ((e = cudaMemcpyAsync(out.data(), digits, N * sizeof(int), cudaMemcpyDeviceToHost, st))) return e;
+    return cudaStreamSynchronize(st);
+}
+
+cudaError_t NttLargeTest::read_ctl(LargeCtl& h, cudaStream_t st) {
+    cudaError_t e = cudaMemcpyAsync(&h, ctl, offsetof(LargeCtl, flags), cudaMemcpyDeviceToHost, st);
+    if (e) return e;
+    return cudaStreamSynchronize(st);
 }
 
 }  // namespace llg

@@ -69,7 +69,7 @@ def lib() -> ctypes.CDLL:
         L.llg_batch_device_ms.argtypes = [ctypes.c_void_p, P(ctypes.c_float)]
         L.llg_batch_destroy.argtypes = [ctypes.c_void_p]
         L.llg_run_noalloc.argtypes = [u64, u64, u32, ctypes.c_void_p, P(dbl), ctypes.c_void_p]
-        L.llg_test_create.argtypes = [u64, u32, P(ctypes.c_void_p)]
+        L.llg_test_create.argtypes = [u64, u32, ctypes.c_int, P(ctypes.c_void_p)]
         L.llg_test_start.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.llg_test_iterate.argtypes = [ctypes.c_void_p, u64, ctypes.c_void_p]
         L.llg_test_read.argtypes = [ctypes.c_void_p, ctypes.c_void_p, P(LlgResult), P(u64), sz]
@@ -201,10 +201,10 @@ class Batch:
 class Test:
     """One exponent on the two-pass engine (llg_test_*): start, iterate on a stream, read."""
 
-    def __init__(self, p, n=0):
+    def __init__(self, p, n=0, engine="fp64"):
         self.p = p
         self.h = ctypes.c_void_p()
-        _check(lib().llg_test_create(p, n, ctypes.byref(self.h)))
+        _check(lib().llg_test_create(p, n, ENGINES[engine], ctypes.byref(self.h)))
 
     def start(self, stream=0):
         _check(lib().llg_test_start(self.h, ctypes.c_void_p(stream or None)))

@@ -110,17 +110,26 @@ def _range_ref(p):
 
 
 def range_(workers: int, hi: int = 100001):
+    """Rows are appended to a partial file as they finish (a restart skips the finished ones);
+    the committed CSV is written once every exponent is done and cross-checked."""
     ps = oracle.primes(2, hi)
-    # largest first, for load balance
-    order = sorted(ps, reverse=True)
-    ctx = mp.get_context("spawn")
+    partial = os.path.join(HERE, ".range_100001.partial")
     rows = {}
+    if os.path.exists(partial):
+        with open(partial) as f:
+            for line in f:
+                p, v, r, h = line.strip().split(",")
+                rows[int(p)] = (v == "1", int(r, 16), h)
+    order = sorted((p for p in ps if p not in rows), reverse=True)  # largest first: load balance
+    ctx = mp.get_context("spawn")
     t0 = time.time()
-    with ctx.Pool(workers) as pool:
+    with ctx.Pool(workers) as pool, open(partial, "a") as out:
         for i, (p, v, r, h) in enumerate(pool.imap_unordered(_range_one, order, chunksize=1)):
             rows[p] = (v, r, h)
+            out.write(f"{p},{int(v)},{r:016x},{h}\n")
+            out.flush()
             if i % 500 == 0:
-                print(f"{i}/{len(ps)} p={p} {time.time() - t0:.0f} s", flush=True)
+                print(f"{len(rows)}/{len(ps)} p={p} {time.time() - t0:.0f} s", flush=True)
         check = [p for p in ps if p <= 30001]
         rng = random.Random(1)
         check += rng.sample([p for p in ps if p > 30001], 400)
@@ -132,6 +141,7 @@ def range_(workers: int, hi: int = 100001):
         for p in ps:
             v, r, h = rows[p]
             f.write(f"{p},{int(v)},{r:016x},{h}\n")
+    os.remove(partial)
 
 
 if __name__ == "__main__":

@@ -65,6 +65,8 @@ def test_test_object_interim_and_errlog(gpu, oracle):
     t = gpu.Test(p, n)
     t.start()
     t.iterate(999)
+    mid = t.read()  # start did the first squaring; reading does not disturb the state
+    assert mid["iters"] == 1000 and mid["res64"] == gpu.run(p, iters=1000, n=n)["res64"]
     t.iterate(1000)
     r = t.read(want_words=True)
     assert r["iters"] == 2000
@@ -91,3 +93,89 @@ def test_large_escalation_exact(gpu, oracle):
     r = gpu.run(p, iters=k, n=65536, want_words=True)
     assert r["status"] == 0 and r["escalations"] >= 1 and r["n"] > 65536
     assert r["words"] == oracle.ll_gmp(p, k)[2]
+
+
+# ---- the two-pass Goldilocks NTT engine (exact: no round-off) ---------------------------------
+
+def _odd_candidate(p):
+    p |= 1
+    while any(p % d == 0 for d in (3, 5, 7, 11, 13)):
+        p -= 2
+    return p
+
+
+@pytest.mark.parametrize("logn", range(14, 24))
+def test_ntt_every_large_length_full_residue(gpu, oracle, logn):
+    """Every two-pass NTT length at its exactness bound ceil(p/N) = (63 - log2 N)/2 (the widest
+    digits the 64-bit field holds), full residue past the first wrap-around."""
+    n = 1 << logn
+    p = _odd_candidate(((63 - logn) // 2) * n - 1)
+    k = p.bit_length() + 4
+    r = gpu.run(p, iters=k, n=n, engine="ntt", want_words=True)
+    assert r["status"] == 0 and r["n"] == n and r["iters"] == k
+    assert r["words"] == oracle.ll_gmp(p, k)[2]
+    assert r["max_err"] == 0.0
+
+
+@pytest.mark.parametrize("logn", [14, 17, 20])
+def test_ntt_large_length_low_digit_floor(gpu, oracle, logn):
+    """The NTT's lowest usable bits per digit (4 floor(p/N) >= log2 N + 12), where the carry
+    chain is longest relative to the digit size."""
+    n = 1 << logn
+    b = -(-(logn + 12) // 4)
+    p = _odd_candidate(b * n + n // 3)
+    k = p.bit_length() + 4
+    r = gpu.run(p, iters=k, n=n, engine="ntt", want_words=True)
+    assert r["status"] == 0 and r["n"] == n
+    assert r["words"] == oracle.ll_gmp(p, k)[2]
+
+
+@pytest.mark.parametrize("p,k", [(1257787, 240), (1257787, 1000), (1257787, 10000)])
+def test_ntt_config_p1257787(gpu, p, k):
+    """p = 1,257,787 on the NTT at its own length (2^16): res64 vs the reference GMP engine."""
+    r = gpu.run(p, iters=k, engine="ntt")
+    assert r["status"] == 0 and r["n"] == 65536
+    assert r["res64"] == _after()[(p, k)]
+
+
+def test_ntt_config_sweep_primes_1000(gpu):
+    g = load_json("appendix.json")
+    after = _after()
+    for p in g["sweep_primes"]:
+        r = gpu.run(p, iters=1000, engine="ntt")
+        assert r["status"] == 0 and r["n"] in (1 << 20, 1 << 21), p
+        assert r["res64"] == after[(p, 1000)], p
+
+
+@pytest.mark.parametrize("k", [34, 1000])
+def test_ntt_config_largest_p136279841(gpu, k):
+    r = gpu.run(136279841, iters=k, engine="ntt")
+    assert r["status"] == 0 and r["n"] == 1 << 23
+    assert r["res64"] == _after()[(136279841, k)]
+
+
+def test_ntt_test_object_pieces(gpu):
+    """llg_test_* on the NTT engine: iterating in pieces equals one run, and equals the FP64
+    engine's residue for the same squarings."""
+    p = 3021377
+    t = gpu.Test(p, 0, engine="ntt")
+    t.start()
+    t.iterate(1)
+    t.iterate(998)
+    mid = t.read()  # start did the first squaring
+    assert mid["iters"] == 1000 and mid["res64"] == gpu.run(p, iters=1000, engine="ntt")["res64"]
+    t.read()  # two reads in a row
+    t.iterate(1000)
+    r = t.read(want_words=True)
+    assert r["iters"] == 2000 and r["max_err"] == 0.0
+    one = gpu.run(p, iters=2000, engine="ntt", want_words=True)
+    f = gpu.run(p, iters=2000, n=1 << 18, want_words=True)
+    assert r["words"] == one["words"] == f["words"]
+    with pytest.raises(gpu.LlgError):
+        t.errlog(10)
+    t.close()
+
+
+def test_ntt_readme_interim_residue(gpu):
+    r = gpu.run(3021377, iters=20000, engine="ntt")
+    assert r["res64"] == 0xCE811E3772129824
