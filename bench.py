@@ -39,6 +39,12 @@ METRIC_RANGE = "tests/s for all p<=100001 (residues exact)"
 BIG_P = 136279841
 METRIC_BIG = "us/LL-iteration at p=136,279,841"
 STEP_ITERS = 1000  # squarings per timed step of the p=136,279,841 workload
+PASS_ITERS = 100   # squarings timed pass by pass for the dominant kernel's roofline
+# DRAM bytes (read + write) of one launch at p=136,279,841, N=2^23, from an ncu capture of
+# `python -m mersenneprime_python_cpp_gmp_benchmark_b200.llgpu square --p 136279841 --iters 6`
+# (profiles/two_pass_p136279841.md). The 64 MiB state is partly L2-resident between the passes.
+NCU_TRAFFIC = {"fp64": {"row": 96642816, "column": 88206080},
+               "ntt": {"row": 118506752, "column": 105664000}}
 
 
 def sieve(lo, hi):
@@ -238,13 +244,13 @@ def bench_range(args, rank, world):
 
 
 def bench_big(args, rank, world):
-    """p = 136,279,841 on the two-pass engine at N = 2^23; one step = 1000 squarings."""
+    """p = 136,279,841 on a two-pass engine at N = 2^23; one step = 1000 squarings."""
     import torch
     from mersenneprime_python_cpp_gmp_benchmark_b200 import llgpu
     n = 1 << 23
     stream = torch.cuda.Stream()
     handle = stream.cuda_stream
-    t = llgpu.Test(BIG_P, n)
+    t = llgpu.Test(BIG_P, n, args.engine)
     t.start(handle)
     flush = L2Flush()
     for _ in range(args.warmup):
@@ -263,7 +269,10 @@ def bench_big(args, rank, world):
             times.append(e0.elapsed_time(e1) * 1e-3)
     torch.cuda.synchronize()
     barrier(world)
-    done = 1 + STEP_ITERS * (args.warmup + args.steps)
+    # the dominant kernel's own time: PASS_ITERS squarings launched one pass at a time, CUDA events
+    # between the launches on the launch stream
+    row_us, col_us = t.time_passes(PASS_ITERS, handle)
+    done = 1 + STEP_ITERS * (args.warmup + args.steps) + PASS_ITERS
     r = t.read(handle)
     assert r["iters"] == done and r["status"] == 0, r
     t.close()
@@ -273,17 +282,23 @@ def bench_big(args, rank, world):
     # correctness of the timed engine: res64 after 1000 squarings vs the reference GMP engine
     gold = {(d["p"], d["k"]): int(d["res64"], 16)
             for d in json.load(open(os.path.join(ROOT, "tests", "golden", "appendix.json")))["after"]}
-    chk = llgpu.run(BIG_P, iters=1000, n=n)
+    chk = llgpu.run(BIG_P, iters=1000, n=n, engine=args.engine)
     assert chk["res64"] == gold[(BIG_P, 1000)], "res64 after 1000 squarings differs from the reference"
     # e2e: the reference-facing call, host in / host out, for a 2000-squaring interim residue
     import lucaslehmer as ll
     k_e2e = 2000
     t0 = time.perf_counter()
-    res64, err = ll.fft_res64_after(BIG_P, k_e2e)
+    if args.engine == "fp64":
+        res64, err = ll.fft_res64_after(BIG_P, k_e2e)
+    else:
+        res64 = ll.gmp_res64_after(BIG_P, k_e2e)  # the exact call; the NTT engine serves it
     t_e2e = time.perf_counter() - t0
     t_e2e = max_over_ranks(t_e2e, world)
     bytes_iter = 32.0 * n   # two read+write sweeps of the 8N-byte state
+    bytes_pass = 16.0 * n   # one pass reads and writes the 8N-byte state once
     flops_iter = 5.0 * n * 23
+    dom, dom_us = ("row", row_us) if row_us >= col_us else ("column", col_us)
+    traffic = NCU_TRAFFIC[args.engine][dom]
     hbm_peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"] \
         if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
     achieved = bytes_iter / (us_iter * 1e-6) / 1e9
@@ -291,20 +306,31 @@ def bench_big(args, rank, world):
     line = {
         "metric": METRIC_BIG, "value": round(us_iter, 3), "unit": "us/iteration", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * t_max / args.steps, 3),
-        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.engine == "fp64" else "u64 (GF(2^64-2^32+1))",
         "data": "synthetic: the LL sequence of p=136,279,841 from s_0=4 (no external data)",
-        "config": {"workload": "p=136,279,841 FP64 IBDWT, N=2^23 (16.25 bits/digit), two-pass "
-                               "(row 1024 x column 4096), 1000 squarings per step",
+        "config": {"workload": ("p=136,279,841 FP64 IBDWT, N=2^23 (16.25 bits/digit), two-pass "
+                                "(row 1024 x column 4096 complex), 1000 squarings per step")
+                   if args.engine == "fp64" else
+                   ("p=136,279,841 Goldilocks NTT IBDWT, N=2^23 (16.25 bits/digit), two-pass "
+                    "(row 1024 x column 8192), 1000 squarings per step"),
+                   "engine": args.engine,
                    "l2": "flushed (512 MiB write) between steps; the 64 MiB state stays on device",
                    "parallelism": f"one independent test per GPU ({world} replica(s))"},
         "e2e": {"value": round(1e6 * t_e2e / k_e2e, 3), "unit": "us/iteration", "iters": k_e2e,
-                "call": "lucaslehmer.fft_res64_after(136279841, 2000): tables, s_0 upload, squarings, "
-                        "digits D2H, exact residue rebuild",
+                "call": ("lucaslehmer.fft_res64_after" if args.engine == "fp64" else "lucaslehmer.gmp_res64_after")
+                        + "(136279841, 2000): tables, s_0 upload, squarings, digits D2H, exact residue rebuild",
                 "h2d_bytes_per_step": 4 * n, "d2h_bytes_per_step": 4 * n},
-        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
-                     "frac": round(achieved / hbm_peak, 4), "peak_source": "MEASURED_PEAKS.json hbm_gbs",
-                     "traffic": None,
-                     "work": "32 N bytes per squaring (two read+write sweeps of the 8N-byte state)"},
+        "roofline": {"bound": "hbm", "achieved": round(bytes_pass / (dom_us * 1e-6) / 1e9, 1), "peak": hbm_peak,
+                     "unit": "GB/s", "frac": round(bytes_pass / (dom_us * 1e-6) / 1e9 / hbm_peak, 4),
+                     "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs, burst copy)",
+                     "traffic": traffic,
+                     "kernel": f"{dom} pass ({'large' if args.engine == 'fp64' else 'ntt'}_{'row' if dom == 'row' else 'col'})",
+                     "kernel_us": round(dom_us, 2), "row_us": round(row_us, 2), "col_us": round(col_us, 2),
+                     "work": "16 N bytes per launch (the 8N-byte state read and written once)",
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch"},
+        "roofline_iteration": {"achieved": round(achieved, 1), "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
+                               "work": "32 N bytes per squaring (two read+write sweeps of the 8N-byte state)"},
         "roofline_fp64": {"achieved": round(flops_iter / (us_iter * 1e-6) / 1e12, 3), "peak": round(fp64_peak, 3),
                           "unit": "TFLOP/s", "frac": round(flops_iter / (us_iter * 1e-6) / 1e12 / fp64_peak, 4),
                           "work": "5 N log2 N flops per squaring", "peak_source": "measured FP64 FMA probe"},
@@ -376,6 +402,7 @@ def main():
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--workload", choices=("big", "range"), default="big")
+    ap.add_argument("--engine", choices=("fp64", "ntt"), default="fp64", help="big workload's engine")
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

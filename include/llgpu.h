@@ -123,6 +123,9 @@ int llg_test_start(llg_test* t, void* stream);
 int llg_test_iterate(llg_test* t, uint64_t iters, void* stream);
 int llg_test_read(llg_test* t, void* stream, llg_result* out, uint64_t* words, size_t nwords);
 int llg_test_errlog(llg_test* t, float* log, size_t cap, size_t* len);
+/* `iters` more squarings launched one pass at a time with CUDA events between the launches (no
+ * graph): the mean device time in microseconds of the row pass and of the column pass. Waits. */
+int llg_test_time_passes(llg_test* t, uint64_t iters, void* stream, double* row_us, double* col_us);
 void llg_test_destroy(llg_test* t);
 
 /* Exact residue of balanced (or any signed) digits: s = sum_j d_j 2^ceil(jp/n) mod 2^p - 1.

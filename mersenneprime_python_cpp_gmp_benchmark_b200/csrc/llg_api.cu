@@ -897,6 +897,14 @@ int llg_test_read(llg_test* t, void* stream, llg_result* out, uint64_t* words, s
     return LLG_OK;
 }
 
+int llg_test_time_passes(llg_test* t, uint64_t iters, void* stream, double* row_us, double* col_us) {
+    if (!t || !row_us || !col_us) return fail(LLG_E_ARG, "null pointer");
+    cudaStream_t st = stream ? (cudaStream_t)stream : default_stream_for_thread();
+    if (t->f) CK(t->f->time_passes(iters, st, *row_us, *col_us));
+    else CK(t->n->time_passes(iters, st, *row_us, *col_us));
+    return LLG_OK;
+}
+
 int llg_test_errlog(llg_test* t, float* log, size_t cap, size_t* len) {
     if (!t || !log) return fail(LLG_E_ARG, "null pointer");
     if (!t->f) return fail(LLG_E_ARG, "the NTT engine has no round-off log (it is exact)");

@@ -47,6 +47,8 @@ struct LargeTest {
     cudaError_t finish(cudaStream_t st, std::vector<int>& out);           // FINAL: digits to host
     cudaError_t read_ctl(LargeCtl& h, cudaStream_t st);
     cudaError_t clear_err_since(cudaStream_t st);
+    // k squarings, one launch at a time with events between the passes: mean device us per pass
+    cudaError_t time_passes(uint64_t k, cudaStream_t st, double& row_us, double& col_us);
 };
 
 // Device state of one exponent on the two-pass NTT engine (same launch sequence as LargeTest).
@@ -67,6 +69,7 @@ struct NttLargeTest {
     cudaError_t step(uint64_t k, cudaStream_t st);
     cudaError_t finish(cudaStream_t st, std::vector<int>& out);
     cudaError_t read_ctl(LargeCtl& h, cudaStream_t st);
+    cudaError_t time_passes(uint64_t k, cudaStream_t st, double& row_us, double& col_us);
 };
 
 bool ntt_large_length_supported(int log_n);

@@ -244,6 +244,50 @@ cudaError_t LargeTest::clear_err_since(cudaStream_t st) {
     return cudaMemsetAsync(&ctl->err_since, 0, sizeof(unsigned long long), st);
 }
 
+namespace {
+
+// Launches k (row, column) pairs with an event after each launch; mean device us of each pass.
+template <class Row, class Col>
+cudaError_t time_pairs(uint64_t k, cudaStream_t st, Row row, Col col, double& row_us, double& col_us) {
+    row_us = col_us = 0.0;
+    if (k == 0) return cudaSuccess;
+    std::vector<cudaEvent_t> ev(2 * k + 1, nullptr);
+    cudaError_t e = cudaSuccess;
+    for (auto& x : ev)
+        if (!e) e = cudaEventCreate(&x);
+    if (!e) e = cudaEventRecord(ev[0], st);
+    for (uint64_t i = 0; i < k && !e; ++i) {
+        e = row();
+        if (!e) e = cudaEventRecord(ev[2 * i + 1], st);
+        if (!e) e = col();
+        if (!e) e = cudaEventRecord(ev[2 * i + 2], st);
+    }
+    if (!e) e = cudaEventSynchronize(ev.back());
+    double r = 0.0, c = 0.0;
+    for (uint64_t i = 0; i < k && !e; ++i) {
+        float a = 0.f, b = 0.f;
+        e = cudaEventElapsedTime(&a, ev[2 * i], ev[2 * i + 1]);
+        if (!e) e = cudaEventElapsedTime(&b, ev[2 * i + 1], ev[2 * i + 2]);
+        r += a;
+        c += b;
+    }
+    for (auto& x : ev)
+        if (x) cudaEventDestroy(x);
+    row_us = 1e3 * r / (double)k;
+    col_us = 1e3 * c / (double)k;
+    return e;
+}
+
+}  // namespace
+
+cudaError_t LargeTest::time_passes(uint64_t k, cudaStream_t st, double& row_us, double& col_us) {
+    cudaError_t e = time_pairs(
+        k, st, [&] { return launch_large_row(logC, LARGE_ITER, args, st); },
+        [&] { return launch_large_col(logR, args, st); }, row_us, col_us);
+    if (!e) done += k;
+    return e;
+}
+
 // Balanced digits of s_0 = 4 (digit 0 holds 4; every digit has >= 3 bits here).
 std::vector<int> seed_digits(uint64_t n) {
     std::vector<int> d(n, 0);
@@ -476,6 +520,14 @@ cudaError_t NttLargeTest::finish(cudaStream_t st, std::vector<int>& out) {
     out.resize(N);
     if ((e = cudaMemcpyAsync(out.data(), digits, N * sizeof(int), cudaMemcpyDeviceToHost, st))) return e;
     return cudaStreamSynchronize(st);
+}
+
+cudaError_t NttLargeTest::time_passes(uint64_t k, cudaStream_t st, double& row_us, double& col_us) {
+    cudaError_t e = time_pairs(
+        k, st, [&] { return launch_ntt_row(logC, LARGE_ITER, args, st); },
+        [&] { return launch_ntt_col(logR, args, st); }, row_us, col_us);
+    if (!e) done += k;
+    return e;
 }
 
 cudaError_t NttLargeTest::read_ctl(LargeCtl& h, cudaStream_t st) {

@@ -299,7 +299,7 @@ __global__ void __launch_bounds__(kNttRowG * (1 << LOG_C) / 16, 2) ntt_row(const
 }
 
 template <int LOG_R>
-__global__ void __launch_bounds__((1 << LOG_R) / 16, 3) ntt_col(const NttLargeArgs A) {
+__global__ void __launch_bounds__((1 << LOG_R) / 16, (LOG_R >= 13 ? 2 : 3)) ntt_col(const NttLargeArgs A) {
     using GR = SmallG<LOG_R>;
     constexpr int R = GR::M, TC = GR::T, E = GR::E;
     constexpr int QL = (int)gl::qpad8_len(R / 4);

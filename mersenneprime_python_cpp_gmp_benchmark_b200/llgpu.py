@@ -74,6 +74,8 @@ def lib() -> ctypes.CDLL:
         L.llg_test_iterate.argtypes = [ctypes.c_void_p, u64, ctypes.c_void_p]
         L.llg_test_read.argtypes = [ctypes.c_void_p, ctypes.c_void_p, P(LlgResult), P(u64), sz]
         L.llg_test_errlog.argtypes = [ctypes.c_void_p, P(ctypes.c_float), sz, P(sz)]
+        L.llg_test_time_passes.argtypes = [ctypes.c_void_p, u64, ctypes.c_void_p, P(ctypes.c_double),
+                                           P(ctypes.c_double)]
         L.llg_test_destroy.argtypes = [ctypes.c_void_p]
         L.llg_test_destroy.restype = None
         L.llg_batch_destroy.restype = None
@@ -223,6 +225,13 @@ class Test:
             d["words"] = list(words)
         return d
 
+    def time_passes(self, iters, stream=0):
+        """`iters` squarings one pass at a time: (mean row-pass us, mean column-pass us)."""
+        r, c = ctypes.c_double(), ctypes.c_double()
+        _check(lib().llg_test_time_passes(self.h, iters, ctypes.c_void_p(stream or None), ctypes.byref(r),
+                                          ctypes.byref(c)))
+        return r.value, c.value
+
     def errlog(self, n):
         buf = (ctypes.c_float * n)()
         ln = ctypes.c_size_t()
@@ -256,3 +265,57 @@ def residue_from_digits(p, n, digits):
     r64, z = ctypes.c_uint64(), ctypes.c_int32()
     _check(lib().llg_residue_from_digits(p, n, d, words, nwords(p), ctypes.byref(r64), ctypes.byref(z)))
     return bool(z.value), r64.value, list(words)
+
+
+def _primes(lo, hi):
+    comp = bytearray(hi + 1)
+    for i in range(2, int(hi ** 0.5) + 1):
+        if not comp[i]:
+            comp[i * i::i] = b"\x01" * len(range(i * i, hi + 1, i))
+    return [i for i in range(max(lo, 2), hi + 1) if not comp[i]]
+
+
+def _main(argv=None):
+    """`python -m mersenneprime_python_cpp_gmp_benchmark_b200.llgpu square|batch ...`: one
+    exponent's squarings on a two-pass engine, or a batch of whole tests; prints one JSON line
+    (res64, worst round-off, wall seconds). Small, self-contained runs for timing and profiling."""
+    import argparse
+    import json
+    import time
+    ap = argparse.ArgumentParser(prog="llgpu")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    a = sub.add_parser("square", help="k squarings of one exponent from s_0 = 4 (llg_test_*)")
+    a.add_argument("--p", type=int, required=True)
+    a.add_argument("--iters", type=int, default=8)
+    a.add_argument("--n", type=int, default=0)
+    a.add_argument("--engine", choices=tuple(ENGINES), default="fp64")
+    b = sub.add_parser("batch", help="whole Lucas-Lehmer tests of every prime in [lo, hi]")
+    b.add_argument("--lo", type=int, required=True)
+    b.add_argument("--hi", type=int, required=True)
+    b.add_argument("--iters", type=int, default=0, help="squarings per test (0 = all p-2)")
+    b.add_argument("--engine", choices=tuple(ENGINES), default="fp64")
+    args = ap.parse_args(argv)
+    t0 = time.perf_counter()
+    if args.cmd == "square":
+        t = Test(args.p, args.n, args.engine)
+        t.start()
+        if args.iters > 1:
+            t.iterate(args.iters - 1)
+        r = t.read()
+        t.close()
+        out = {"p": args.p, "n": r["n"], "iters": r["iters"], "res64": f"{r['res64']:016x}",
+               "max_err": r["max_err"], "engine": args.engine}
+    else:
+        ps = _primes(args.lo, args.hi)
+        rs = run_batch(ps, args.iters, args.engine)
+        out = {"tests": len(ps), "hits": [r["p"] for r in rs if r["is_zero"]],
+               "failed": [r["p"] for r in rs if r["status"]], "engine": args.engine,
+               "lengths": sorted({r["n"] for r in rs})}
+    out["seconds"] = round(time.perf_counter() - t0, 3)
+    print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    import sys
+    sys.exit(_main())
