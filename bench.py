@@ -135,23 +135,13 @@ def barrier(world):
 
 
 def max_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from mersenneprime_python_cpp_gmp_benchmark_b200 import replicas
+    return replicas.reduce_max(x) if world > 1 else x
 
 
 def sum_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    from mersenneprime_python_cpp_gmp_benchmark_b200 import replicas
+    return replicas.reduce_sum(x) if world > 1 else x
 
 
 class L2Flush:
@@ -183,7 +173,8 @@ def bench_range(args, rank, world):
     import torch
     from mersenneprime_python_cpp_gmp_benchmark_b200 import llgpu
     ps_all = sieve(2, RANGE_HI)
-    mine = sorted(ps_all, reverse=True)[rank::world]  # round-robin over descending p: balanced shards
+    from mersenneprime_python_cpp_gmp_benchmark_b200 import replicas
+    mine = replicas.shard(ps_all, rank, world)  # independent tests, balanced by squaring cost
     batch = llgpu.Batch(mine)
     flush = L2Flush()
     for _ in range(args.warmup):
@@ -230,7 +221,7 @@ def bench_range(args, rank, world):
         "config": {"workload": "range p<=100001 (9592 LL tests, batched whole-test kernels, FP64 IBDWT, "
                                "pow2 N 32..8192 at <=18 bits/digit)",
                    "tests": len(ps_all), "l2": "flushed (512 MiB write) between steps",
-                   "parallelism": f"exponents sharded round-robin over {world} GPU(s)"},
+                   "parallelism": f"independent tests split over {world} GPU(s) by squaring cost (replicas)"},
         "e2e": {"value": round(e2e, 2), "unit": "tests/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "fp64", "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "TFLOP/s",
                      "frac": round(achieved / peak, 4),
@@ -278,7 +269,8 @@ def bench_big(args, rank, world):
     t.close()
     t_rank = sum(times)
     t_max = max_over_ranks(t_rank, world)
-    us_iter = 1e6 * t_max / (STEP_ITERS * args.steps)
+    # whole job: `world` independent replicas each did STEP_ITERS * steps squarings in <= t_max
+    us_iter = 1e6 * t_max / (STEP_ITERS * args.steps * world)
     # correctness of the timed engine: res64 after 1000 squarings vs the reference GMP engine
     gold = {(d["p"], d["k"]): int(d["res64"], 16)
             for d in json.load(open(os.path.join(ROOT, "tests", "golden", "appendix.json")))["after"]}
@@ -301,7 +293,7 @@ def bench_big(args, rank, world):
     traffic = NCU_TRAFFIC[args.engine][dom]
     hbm_peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"] \
         if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
-    achieved = bytes_iter / (us_iter * 1e-6) / 1e9
+    achieved = bytes_iter / (us_iter * world * 1e-6) / 1e9  # per GPU
     fp64_peak = llgpu.measure_peak("fp64") / 1e12
     line = {
         "metric": METRIC_BIG, "value": round(us_iter, 3), "unit": "us/iteration", "n_gpus": world,
@@ -331,8 +323,9 @@ def bench_big(args, rank, world):
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch"},
         "roofline_iteration": {"achieved": round(achieved, 1), "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
                                "work": "32 N bytes per squaring (two read+write sweeps of the 8N-byte state)"},
-        "roofline_fp64": {"achieved": round(flops_iter / (us_iter * 1e-6) / 1e12, 3), "peak": round(fp64_peak, 3),
-                          "unit": "TFLOP/s", "frac": round(flops_iter / (us_iter * 1e-6) / 1e12 / fp64_peak, 4),
+        "roofline_fp64": {"achieved": round(flops_iter / (us_iter * world * 1e-6) / 1e12, 3),
+                          "peak": round(fp64_peak, 3), "unit": "TFLOP/s",
+                          "frac": round(flops_iter / (us_iter * world * 1e-6) / 1e12 / fp64_peak, 4),
                           "work": "5 N log2 N flops per squaring", "peak_source": "measured FP64 FMA probe"},
         "max_roundoff": r["max_err"],
         "clocks": clk.summary(),

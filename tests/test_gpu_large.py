@@ -179,3 +179,29 @@ def test_ntt_test_object_pieces(gpu):
 def test_ntt_readme_interim_residue(gpu):
     r = gpu.run(3021377, iters=20000, engine="ntt")
     assert r["res64"] == 0xCE811E3772129824
+
+
+@pytest.mark.parametrize("engine", ["fp64", "ntt"])
+def test_config_p1257787_full_run_trace(gpu, engine):
+    """p = 1,257,787 (a Mersenne exponent) at N = 65536, all 1,257,785 squarings: res64 every 10^4
+    squarings equals the GMP trace (tests/golden/trace_1257787.json), the final residue is zero, and
+    (FP64) the worst round-off over the run, and of every logged squaring, stays <= 0.4."""
+    tr = load_json("trace_1257787.json")
+    p, every = tr["p"], tr["every"]
+    t = gpu.Test(p, 65536, engine)
+    t.start()
+    done = 1
+    for i, want in enumerate(tr["res64"]):
+        k = every * (i + 1)
+        t.iterate(k - done)
+        done = k
+        r = t.read()
+        assert r["iters"] == k and r["res64"] == int(want, 16), (engine, k)
+    t.iterate(p - 2 - done)
+    r = t.read()
+    assert r["iters"] == p - 2 and r["is_zero"] and r["res64"] == 0
+    assert r["status"] == 0 and r["max_err"] <= 0.4
+    if engine == "fp64":
+        log = t.errlog(65536)
+        assert len(log) == 65536 and 0.0 < max(log) <= r["max_err"] + 1e-7
+    t.close()
