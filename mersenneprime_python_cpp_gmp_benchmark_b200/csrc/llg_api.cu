@@ -9,6 +9,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -17,6 +18,7 @@
 
 #include "../../include/llgpu.h"
 #include "llg_host.h"
+#include "llg_device.cuh"
 #include "llg_internal.h"
 
 namespace {
@@ -108,7 +110,8 @@ int device_ready(int* dev_out) {
     return LLG_OK;
 }
 
-// e^{-2 pi i r / M}, r < M/4, rounded once from long double, stored at qpad(r).
+// e^{-2 pi i r / M}, r < M/4, rounded once from long double, stored at qpad(r) (the whole-test
+// kernel's quarter-wave table).
 std::vector<double2> quarter_table(int log_m) { return padded_quarter_table((uint64_t)1 << log_m); }
 
 int get_qtw(int dev, int log_m, const double2** out) {
@@ -408,6 +411,18 @@ double bits_to_double(unsigned long long b) {
     return d;
 }
 
+// Row length of the two-pass FP64 engine per log2 N (-1: the built-in default); set by
+// llg_set_large_split (the autotuner's choice).
+std::atomic<int> g_large_log_c[kLargeLogMax + 1];
+struct SplitInit {
+    SplitInit() {
+        for (auto& x : g_large_log_c) x.store(-1);
+    }
+} g_split_init;
+
+cudaError_t init_large(LargeTest& T, uint64_t p, int l) { return T.init(p, l, g_large_log_c[l].load()); }
+cudaError_t init_large(NttLargeTest& T, uint64_t p, int l) { return T.init(p, l); }
+
 template <class TestT>
 int run_large_t(const Item& item, llg_result& r, std::vector<uint64_t>* words, cudaStream_t st) {
     uint32_t n = item.n;
@@ -417,7 +432,7 @@ int run_large_t(const Item& item, llg_result& r, std::vector<uint64_t>* words, c
     CK(cudaEventCreate(&e1));
     for (;;) {
         TestT T;
-        CK(T.init(item.p, ilog2_exact(n)));
+        CK(init_large(T, item.p, ilog2_exact(n)));
         CK(cudaEventRecord(e0, st));
         CK(T.start(seed_digits(n), st));
         uint64_t left = item.iters - 1;
@@ -545,6 +560,9 @@ int make_batch(const uint64_t* ps, size_t count, uint64_t max_iters, int engine,
         Group g;
         g.n = kv.first;
         g.items = std::move(kv.second);
+        // longest tests first: blocks start in index order, so the last wave holds the short ones
+        std::stable_sort(g.items.begin(), g.items.end(),
+                         [](const Item& x, const Item& y) { return x.iters > y.iters; });
         b->groups.push_back(std::move(g));
     }
     // largest lengths first (they run longest)
@@ -703,6 +721,20 @@ uint32_t llg_fft_length(uint64_t p, double max_bpw) {
     return fp64_length(p, max_bpw);
 }
 
+int llg_set_large_split(int log_n, int log_c) {
+    if (!large_length_supported(log_n)) return fail(LLG_E_ARG, "log2 N = %d is not a two-pass length", log_n);
+    if (log_c >= 0 && !large_split_supported(log_n, log_c))
+        return fail(LLG_E_UNSUPPORTED, "no kernels for rows of 2^%d at N = 2^%d", log_c, log_n);
+    g_large_log_c[log_n].store(log_c < 0 ? -1 : log_c);
+    return LLG_OK;
+}
+
+int llg_get_large_split(int log_n) {
+    if (!large_length_supported(log_n)) return -1;
+    const int v = g_large_log_c[log_n].load();
+    return v >= 0 ? v : large_default_log_c(log_n);
+}
+
 int llg_set_max_bpw(double b) {
     if (!(b >= 2.0 && b <= (double)kMaxDigitBits)) return fail(LLG_E_ARG, "bits per word %g out of range [2, 28]", b);
     g_max_bpw = b;
@@ -840,7 +872,7 @@ int llg_test_create(uint64_t p, uint32_t n, int engine, llg_test** out) {
         e = t->n->init(p, l);
     } else {
         t->f.reset(new llg::LargeTest());
-        e = t->f->init(p, l);
+        e = init_large(*t->f, p, l);
     }
     if (e != cudaSuccess) {
         delete t;

@@ -170,6 +170,28 @@ __device__ __forceinline__ double i2d_shift(long long x) {
     return __dsub_rn(__longlong_as_double(x + 0x4338000000000000LL), SH);
 }
 
+// 2^e as a double (normal range).
+__device__ __forceinline__ double pow2(int e) { return __longlong_as_double((long long)(1023 + e) << 52); }
+
+// Balanced split of an integer-valued double: v = x + c 2^b with |x| <= 2^(b-1) (ties to even),
+// c and x exact for |v| < 2^51; inv = 2^-b, pw = 2^b. The FP64 form of the reference's carry step
+// (lucaslehmer.cpp:299-303: c = floor((v + 2^(b-1)) / 2^b)); the two differ only at ties, and
+// either representation of the residue is exact.
+__device__ __forceinline__ double dsplit(double v, double inv, double pw, double& c) {
+    constexpr double SH = 6755399441055744.0;  // 1.5 * 2^52: adding it rounds to an integer
+    c = __dsub_rn(__fma_rn(v, inv, SH), SH);
+    return __fma_rn(-c, pw, v);
+}
+
+// dsplit with digit size e bits: 2^e and 2^-e built from the exponent field (few live registers).
+__device__ __forceinline__ double dsplit_e(double v, int e, double& c) {
+    const double pw = __hiloint2double((1023 + e) << 20, 0), inv = __hiloint2double((1023 - e) << 20, 0);
+    return dsplit(v, inv, pw, c);
+}
+
+// An integer-valued double with |x| < 2^31 as int32 (the low word of x + 1.5 * 2^52).
+__device__ __forceinline__ int d2i_exact(double x) { return __double2loint(__dadd_rn(x, 6755399441055744.0)); }
+
 // One balanced-digit step: v = x + carry_in; returns the digit in [-2^(b-1), 2^(b-1)) and sets
 // carry = floor((v + 2^(b-1)) / 2^b)  (lucaslehmer.cpp:299-303).
 __device__ __forceinline__ long long balance(long long v, int b, long long& carry) {

@@ -15,6 +15,11 @@
 
 namespace llg {
 
+// Twiddle table of a geometry: e^{-2 pi i r / M} at slot qpad(r) for r < M/4 (TW_QUARTER: the
+// other quadrants by rotation), r < M/2 (TW_HALF: the other half by negation), or r < M (TW_FULL:
+// one table read, no fold).
+enum { TW_QUARTER = 0, TW_HALF = 1, TW_FULL = 2 };
+
 // L = 2^LOG_M points, E = 2^LOG_E values per thread (radix-E passes, the last one RLAST).
 template <int LOG_M, int LOG_E = 4>
 struct SmallGeom {
@@ -74,6 +79,22 @@ struct NamedSync {
     }
 };
 
+// Twiddle e^{-2 pi i x / M} (conjugated when inv) for geometry G, from its table.
+template <class G>
+__device__ __forceinline__ double2 twiddle_g(const double2* __restrict__ q, uint32_t x, bool inv) {
+    if constexpr (G::TWM == TW_FULL) {
+        const double2 w = q[qpad(x & (uint32_t)(G::M - 1))];
+        return inv ? conj2(w) : w;
+    } else if constexpr (G::TWM == TW_HALF) {
+        constexpr uint32_t H = (uint32_t)G::M / 2;
+        const double2 w = q[qpad(x & (H - 1))];
+        const bool ng = (x & H) != 0;  // e^{-2 pi i (r + M/2) / M} = -e^{-2 pi i r / M}
+        return make_double2(ng ? -w.x : w.x, (ng != inv) ? -w.y : w.y);
+    } else {
+        return twiddle<G::LOG_M_>(q, x, inv);
+    }
+}
+
 // Forward (INV=false) or inverse radix pass S on the register array v (E values).
 // Forward: load (S > 0), DFT, twiddle w_L^{n2 k1}, store (S < P-1).
 // Inverse: load (S < P-1), conj twiddle, inverse DFT, store (S > 0).
@@ -86,16 +107,22 @@ __device__ __forceinline__ void radix_pass(double2 (&v)[G::E], double2* __restri
     constexpr int B = G::E / R;
     constexpr bool LOAD = INV ? (S < G::P - 1) : (S > 0);
     constexpr bool STORE = INV ? (S > 0) : (S < G::P - 1);
+    // phys(base + n1 ST) = phys(base) + n1 * DST whenever the R slots of a butterfly never cross a
+    // 16-slot boundary out of step with base: ST a multiple of 16, or the whole group (L slots,
+    // 16-aligned) inside one 16-slot block. The offsets are then compile-time constants.
+    constexpr bool AFFINE = (ST % 16 == 0) || (L <= 16);
+    constexpr int DST = (ST % 16 == 0) ? ST + ST / 16 : ST;
 #pragma unroll
     for (int h = 0; h < B; ++h) {
         const int beta = t * B + h;
         const int g = beta / ST, n2 = beta % ST;
         const int base = g * L + n2;
+        const int pbase = phys(base);
         double2* vv = v + h * R;
         if constexpr (LOAD) {
 #pragma unroll
             for (int n1 = 0; n1 < R; ++n1) {
-                const int x = phys(base + n1 * ST);
+                const int x = AFFINE ? pbase + n1 * DST : phys(base + n1 * ST);
                 vv[n1] = buf[x];
             }
         }
@@ -104,20 +131,20 @@ __device__ __forceinline__ void radix_pass(double2 (&v)[G::E], double2* __restri
             if constexpr (ST > 1) {
 #pragma unroll
                 for (int k1 = 1; k1 < R; ++k1)
-                    vv[k1] = cmul(vv[k1], twiddle<G::LOG_M_>(qtw, (uint32_t)(n2 * k1) << (G::LE * S), false));
+                    vv[k1] = cmul(vv[k1], twiddle_g<G>(qtw, (uint32_t)(n2 * k1) << (G::LE * S), false));
             }
         } else {
             if constexpr (ST > 1) {
 #pragma unroll
                 for (int k1 = 1; k1 < R; ++k1)
-                    vv[k1] = cmul(vv[k1], twiddle<G::LOG_M_>(qtw, (uint32_t)(n2 * k1) << (G::LE * S), true));
+                    vv[k1] = cmul(vv[k1], twiddle_g<G>(qtw, (uint32_t)(n2 * k1) << (G::LE * S), true));
             }
             Dft<R, true>::run(vv);
         }
         if constexpr (STORE && !SYNC_BEFORE_STORE) {
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1) {
-                const int x = phys(base + k1 * ST);
+                const int x = AFFINE ? pbase + k1 * DST : phys(base + k1 * ST);
                 buf[x] = vv[k1];
             }
         }
@@ -129,9 +156,10 @@ __device__ __forceinline__ void radix_pass(double2 (&v)[G::E], double2* __restri
             const int beta = t * B + h;
             const int g = beta / ST, n2 = beta % ST;
             const int base = g * L + n2;
+            const int pbase = phys(base);
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1) {
-                const int x = phys(base + k1 * ST);
+                const int x = AFFINE ? pbase + k1 * DST : phys(base + k1 * ST);
                 buf[x] = v[h * R + k1];
             }
         }
@@ -162,9 +190,16 @@ __device__ __forceinline__ void inverse_from(double2 (&v)[G::E], double2* buf, c
     }
 }
 
-template <int LOG_M_T, int LOG_E = 4>
+template <int LOG_M_T, int LOG_E = 4, int TW = TW_QUARTER>
 struct SmallG : SmallGeom<LOG_M_T, LOG_E> {
     static constexpr int LOG_M_ = LOG_M_T;
+    static constexpr int TWM = TW;
 };
+
+// Length (16-byte slots) of the twiddle table a geometry reads.
+template <class G>
+__host__ __device__ constexpr uint32_t twiddle_table_len() {
+    return qpad_len((uint32_t)G::M >> (G::TWM == TW_FULL ? 0 : G::TWM == TW_HALF ? 1 : 2));
+}
 
 }  // namespace llg

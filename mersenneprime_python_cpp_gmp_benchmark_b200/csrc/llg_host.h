@@ -13,6 +13,8 @@ namespace llg {
 constexpr int kGraphChunk = 64;  // squarings per captured CUDA graph
 
 bool large_length_supported(int log_n);
+int large_default_log_c(int log_n);
+bool large_split_supported(int log_n, int log_c);
 int set_error(int code, const char* msg);  // records this thread's llg_last_error() text
 cudaError_t configure_large(int log_c, int log_r);
 std::vector<int> seed_digits(uint64_t n);
@@ -25,8 +27,9 @@ struct LargeTest {
     uint64_t p = 0, M = 0;
     int logN = 0, logC = 0, logR = 0, C = 0, R = 0, nblocks = 0;
     double2* V = nullptr;
-    long long* carry = nullptr;
-    int* carry2 = nullptr;
+    double* carry = nullptr;
+    float* carry2 = nullptr;
+    double* halo = nullptr;
     LargeCtl* ctl = nullptr;
     int* digits = nullptr;
     float* errlog = nullptr;
@@ -40,7 +43,7 @@ struct LargeTest {
     uint64_t done = 0;  // squarings enqueued since start()
 
     ~LargeTest();
-    cudaError_t init(uint64_t p, int log_n);
+    cudaError_t init(uint64_t p, int log_n, int log_c = -1);              // log_c < 0: default split
     cudaError_t start(const std::vector<int>& digits, cudaStream_t st);  // INIT + first squaring
     cudaError_t step(uint64_t k, cudaStream_t st);                        // k more squarings
     cudaError_t step_plain(uint64_t k, bool dump_last, cudaStream_t st);

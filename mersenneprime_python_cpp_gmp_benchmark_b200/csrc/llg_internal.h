@@ -45,7 +45,12 @@ cudaError_t launch_small_ntt(int log_n, const SmallJob* jobs, int njobs, const u
 
 // ---- two-pass engine (N = 2^16 .. 2^23): state resident in HBM ------------------------------
 
-constexpr int kRowG = 4;              // rows per row-pass block
+constexpr int kRowG = 4;              // rows per row-pass block (rows of up to 1024 complex)
+// rows per row-pass block for a row length of 2^log_c complex values (64 KiB of state per block)
+#ifdef __CUDACC__
+__host__ __device__
+#endif
+constexpr int large_rows_per_block(int log_c) { return log_c >= 11 ? 2 : kRowG; }
 constexpr int kLargeLogE = 4;         // log2 of the complex values per thread in the two-pass kernels
 constexpr int kLargeMaxBlocks = 1024; // row blocks (R / kRowG) supported by the control block
 
@@ -81,7 +86,7 @@ __device__ __forceinline__ void wait_flag(unsigned int* f, unsigned int target, 
 
 struct LargeArgs {
     double2* V;               // state: element (row a, column slot pos) at pos * R + a
-    const double2* qtwC;      // quarter table of the C-point row FFT
+    const double2* qtwC;      // full padded twiddle table of the C-point row FFT
     const double2* qtwR;      // quarter table of the R-point column FFT
     const double2* tw1;       // e^{-2 pi i x / M}, x < 2^tw_shift
     const double2* tw2;       // e^{-2 pi i y 2^tw_shift / M}
@@ -92,8 +97,9 @@ struct LargeArgs {
     const double* wB;         // [C] 2^(sB/N)
     const double* iwB;        // [C] 2^(-sB/N) / (4M)
     const int* sB;            // [C] (-2Rb p) mod N
-    long long* carry;         // [nblocks][C] hop-1 carry-outs of each block's last row
-    int* carry2;              // [nblocks][C] hop-2 carry-outs of each block's last row
+    double* carry;            // [nblocks][C] hop-1 carry-outs of each block's last row (integers)
+    float* carry2;            // [nblocks][C] hop-2 carry-outs (integers of a few units)
+    double* halo;             // [2][C] block 0's wrap-around carries (hop 2, hop 3)
     LargeCtl* ctl;
     int* digits;              // N int32, natural order (INIT input; dump / FINAL output)
     float* errlog;            // per-epoch max round-off ring (may be null)

@@ -54,19 +54,19 @@ __device__ __forceinline__ double2 twiddle_M(const LargeArgs& A, uint32_t x, boo
 }  // namespace
 
 template <int LOG_C, int MODE>
-__global__ void __launch_bounds__(kRowG * (1 << LOG_C) / (1 << kLargeLogE), 2) large_row(const LargeArgs A) {
-    using GC = SmallG<LOG_C, kLargeLogE>;
-    constexpr int C = GC::M, TR = GC::T, E = GC::E, G = kRowG, T = G * TR;
+__global__ void __launch_bounds__(large_rows_per_block(LOG_C) * (1 << LOG_C) / (1 << kLargeLogE), 2)
+    large_row(const LargeArgs A) {
+    using GC = SmallG<LOG_C, kLargeLogE, TW_FULL>;  // full twiddle table
+    constexpr int C = GC::M, TR = GC::T, E = GC::E, G = large_rows_per_block(LOG_C), T = G * TR;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int RS = GC::PAD + 1;  // row-buffer stride: odd, so the 8 rows of a slot hit 8 banks
-    double2* bufs = reinterpret_cast<double2*>(smem_raw);        // G exchange buffers of RS slots
-    double2* qtw = bufs + G * RS;                                  // padded quarter table (C-point)
-    constexpr int QL = (int)qpad_len(C / 4);
-    long long* hin = reinterpret_cast<long long*>(qtw + QL);      // C: wrap carry into row 0 (hop 2)
-    long long* hc1 = hin + C;                                     // C: row R-2's carry-out (block 0)
-    int* hin2 = reinterpret_cast<int*>(hc1 + C);                  // C: wrap carry into row 0 (hop 3)
-    long long* carr = reinterpret_cast<long long*>(bufs);         // G x C hop-1 carry-outs (reuses bufs)
-    int* carr2 = reinterpret_cast<int*>(carr + G * C);            // G x C hop-2 carry-outs
+    constexpr int RS = GC::PAD + 1;  // row-buffer stride: odd, so the rows of a slot hit different banks
+    constexpr int QL = (int)twiddle_table_len<GC>();
+    double2* bufs = reinterpret_cast<double2*>(smem_raw);  // G exchange buffers of RS slots
+    double2* qtw = bufs + G * RS;                            // padded twiddle table (C-point)
+    double* carr = reinterpret_cast<double*>(bufs);          // G x C hop-1 carry-outs (reuses bufs)
+    double* carr2 = carr + G * C;                            // G x C hop-2 carry-outs
+    double* hin = reinterpret_cast<double*>(A.halo);         // C: wrap carry into row 0 (hop 2)
+    double* hin2 = hin + C;                                  // C: wrap carry into row 0 (hop 3)
     __shared__ unsigned long long s_err;
     __shared__ int s_blk;
     __shared__ unsigned s_epoch;
@@ -101,13 +101,11 @@ __global__ void __launch_bounds__(kRowG * (1 << LOG_C) / (1 << kLargeLogE), 2) l
     const unsigned ep = s_epoch;
     const int a0 = blk * G;
     const int a = a0 + rg;
+    // digit sizes: b = q or q + 1 bits, as 2^b and 2^-b
+    const double pw0 = pow2(A.q), pw1 = pow2(A.q + 1), iv0 = pow2(-A.q), iv1 = pow2(-A.q - 1);
 
     double2 v[E];
-    int x0s[E], x1s[E];
-    double lerr = 0.0;
-
-    // per-row weight halves (digits 2a and 2a+1)
-    const int sA0 = __ldg(A.sA + 2 * a), sA1 = __ldg(A.sA + 2 * a + 1);
+    double x0s[E], x1s[E];
 
     if constexpr (MODE == LARGE_INIT) {
 #pragma unroll
@@ -115,186 +113,165 @@ __global__ void __launch_bounds__(kRowG * (1 << LOG_C) / (1 << kLargeLogE), 2) l
             const int b = tr + TR * i;
             const size_t m = (size_t)a + (size_t)R * b;
             const int2 d = *reinterpret_cast<const int2*>(A.digits + 2 * m);
-            x0s[i] = d.x;
-            x1s[i] = d.y;
+            x0s[i] = (double)d.x;
+            x1s[i] = (double)d.y;
         }
     } else {
-        // ---- wrap-around carries into row 0 (2^p == 1): block 0 recomputes rows R-2 (row group 0)
-        //      and R-1 (the other row groups, which keeps the FFT's barriers uniform) side by side.
-        //      Row R-1, column b feeds row 0, column b+1; column C-1 wraps to digit 0. ----
-        if (blk == 0) {
-            const int ah = R - 2 + (rg > 0 ? 1 : 0);
+        double lerr = 0.0;
+        // Phase 0 (block 0 only): the last block's rows R-G .. R-1 through the same inverse FFT
+        // and hops 1-2, for the carry-outs of row R-1 that wrap into row 0 (2^p == 1), exactly as
+        // the last block computes and publishes them. Phase 1: the block's own rows.
+#pragma unroll 1
+        for (int ph = (blk == 0) ? 0 : 1; ph < 2; ++ph) {
+            const int base = ph ? a0 : R - G;
+            const int ar = base + rg;
+            // ---- load rows base .. base+G-1 (coalesced: G contiguous values per column slot) ----
+            {
+                double2 tmp[G * C / T];
 #pragma unroll
-            for (int j = 0; j < E; ++j) v[j] = A.V[(size_t)(tr * E + j) * R + ah];
-            inverse_from<GC, GC::P - 1, false>(v, buf, qtw, tr, gsync);
+                for (int r = 0; r < G * C / T; ++r) {
+                    const int qq = t + T * r, pos = qq / G, ra = qq % G;
+                    tmp[r] = A.V[(size_t)pos * R + base + ra];
+                }
+#pragma unroll
+                for (int r = 0; r < G * C / T; ++r) {
+                    const int qq = t + T * r, pos = qq / G, ra = qq % G;
+                    bufs[ra * RS + phys(pos)] = tmp[r];
+                }
+            }
             __syncthreads();
-            if (t == 0) {
-                // rows R-2 and R-1 are read: the last block may overwrite them
+            if (ph == 0 && t == 0) {
+                // rows R-G .. R-1 are read: the last block may overwrite them
                 __threadfence();
                 *reinterpret_cast<volatile unsigned*>(&A.ctl->halo_read) = ep + 1u;
             }
-            const int h0 = __ldg(A.sA + 2 * ah), h1 = __ldg(A.sA + 2 * ah + 1);
-            const double ih0 = __ldg(A.iwA + 2 * ah), ih1 = __ldg(A.iwA + 2 * ah + 1);
-            long long hc[E];
+#pragma unroll
+            for (int j = 0; j < E; ++j) v[j] = buf[phys(tr * E + j)];
+            inverse_from<GC, GC::P - 1, false>(v, buf, qtw, tr, gsync);
+            __syncthreads();  // the exchange buffers become the carry arrays
+
+            // ---- hop 1: unweight, round, round-off, two-digit chain per (row, column) from zero;
+            //      the carry-out goes to the next row. ----
+            const int sA0 = __ldg(A.sA + 2 * ar), sA1 = __ldg(A.sA + 2 * ar + 1);
+            const double ia0 = __ldg(A.iwA + 2 * ar), ia1 = __ldg(A.iwA + 2 * ar + 1);
 #pragma unroll
             for (int i = 0; i < E; ++i) {
                 const int b = tr + TR * i;
                 const int sb = __ldg(A.sB + b);
                 const double iwb = __ldg(A.iwB + b);
-                const bool o0 = h0 + sb >= N, o1 = h1 + sb >= N;
-                const int s0 = o0 ? h0 + sb - N : h0 + sb, s1 = o1 ? h1 + sb - N : h1 + sb;
-                const int b0 = A.q + (s0 < A.rem), b1 = A.q + (s1 < A.rem);
-                const double va = v[i].x * (ih0 * iwb) * (o0 ? 2.0 : 1.0);
-                const double vb = v[i].y * (ih1 * iwb) * (o1 ? 2.0 : 1.0);
-                long long la, lb, c;
-                const double ra = round_shift(va, la), rb = round_shift(vb, lb);
+                const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
+                const int s0 = o0 ? sA0 + sb - N : sA0 + sb, s1 = o1 ? sA1 + sb - N : sA1 + sb;
+                const bool w0 = s0 < A.rem, w1 = s1 < A.rem;  // digit of q + 1 bits
+                const double va = v[i].x * (ia0 * iwb) * (o0 ? 2.0 : 1.0);
+                const double vb = v[i].y * (ia1 * iwb) * (o1 ? 2.0 : 1.0);
+                long long ia, ib;
+                const double ra = round_shift(va, ia), rb = round_shift(vb, ib);
                 lerr = fmax(lerr, fmax(fabs(va - ra), fabs(vb - rb)));
-                x0s[i] = (int)balance(la, b0, c);
-                x1s[i] = (int)balance(lb + c, b1, c);
-                hc[i] = c;
-                if (rg == 0) hc1[b] = c;
+                double c;
+                x0s[i] = dsplit(ra, w0 ? iv1 : iv0, w0 ? pw1 : pw0, c);
+                x1s[i] = dsplit(rb + c, w1 ? iv1 : iv0, w1 ? pw1 : pw0, c);
+                carr[rg * C + b] = c;
             }
+            atomicMax(&s_err, (unsigned long long)__double_as_longlong(lerr));
             __syncthreads();
-            if (rg == 1) {
-                // second hop of row R-1 with row R-2's carry-out (same column)
+            // ---- hop 2 for rows fed from inside the block ----
+            if (rg > 0) {
 #pragma unroll
                 for (int i = 0; i < E; ++i) {
                     const int b = tr + TR * i;
                     const int sb = __ldg(A.sB + b);
-                    const bool o0 = h0 + sb >= N, o1 = h1 + sb >= N;
-                    const int s0 = o0 ? h0 + sb - N : h0 + sb, s1 = o1 ? h1 + sb - N : h1 + sb;
-                    const int b0 = A.q + (s0 < A.rem), b1 = A.q + (s1 < A.rem);
-                    long long c;
-                    const long long x0 = balance((long long)x0s[i] + hc1[b], b0, c);
-                    balance((long long)x1s[i] + c, b1, c);
-                    (void)x0;
-                    hin[(b + 1) & (C - 1)] = hc[i];
-                    hin2[(b + 1) & (C - 1)] = (int)c;
+                    const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
+                    const int s0 = o0 ? sA0 + sb - N : sA0 + sb, s1 = o1 ? sA1 + sb - N : sA1 + sb;
+                    const bool w0 = s0 < A.rem, w1 = s1 < A.rem;
+                    double c;
+                    x0s[i] = dsplit(x0s[i] + carr[(rg - 1) * C + b], w0 ? iv1 : iv0, w0 ? pw1 : pw0, c);
+                    x1s[i] = dsplit(x1s[i] + c, w1 ? iv1 : iv0, w1 ? pw1 : pw0, c);
+                    carr2[rg * C + b] = c;
+                }
+            }
+            if (ph == 0) {
+                // row R-1, column b feeds row 0, column b+1; column C-1 wraps to digit 0
+                if (rg == G - 1) {
+#pragma unroll
+                    for (int i = 0; i < E; ++i) {
+                        const int b = tr + TR * i;
+                        hin[(b + 1) & (C - 1)] = carr[(G - 1) * C + b];
+                        hin2[(b + 1) & (C - 1)] = carr2[(G - 1) * C + b];
+                    }
+                }
+                __syncthreads();  // carry arrays read before phase 1 reloads the buffers
+                continue;
+            }
+            if (rg == G - 1) {
+#pragma unroll
+                for (int i = 0; i < E; ++i) {
+                    const int b = tr + TR * i;
+                    A.carry[(size_t)blk * C + b] = carr[(G - 1) * C + b];
+                    A.carry2[(size_t)blk * C + b] = (float)carr2[(G - 1) * C + b];
+                }
+            }
+            __threadfence();  // each writer orders its carry-out stores before the flag below
+            __syncthreads();
+            if (t == 0) {
+                __threadfence();
+                *reinterpret_cast<volatile unsigned*>(&A.ctl->flags[blk]) = ep + 1u;
+                if (blk > 0) wait_flag(&A.ctl->flags[blk - 1], ep + 1u, A.ctl, kSpinLimit);  // block blk-1's carries
+            }
+            __syncthreads();
+            // ---- hop 2 for the block's first row: previous block's last row, or the wrap ----
+            if (rg == 0) {
+#pragma unroll
+                for (int i = 0; i < E; ++i) {
+                    const int b = tr + TR * i;
+                    double cin = (blk > 0) ? __ldcg(A.carry + (size_t)(blk - 1) * C + b) : hin[b];
+                    if (a == 0 && b == 0) cin -= 2.0;  // the "- 2" of s^2 - 2 (digit 0)
+                    const int sb = __ldg(A.sB + b);
+                    const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
+                    const int s0 = o0 ? sA0 + sb - N : sA0 + sb, s1 = o1 ? sA1 + sb - N : sA1 + sb;
+                    const bool w0 = s0 < A.rem, w1 = s1 < A.rem;
+                    double c;
+                    x0s[i] = dsplit(x0s[i] + cin, w0 ? iv1 : iv0, w0 ? pw1 : pw0, c);
+                    x1s[i] = dsplit(x1s[i] + c, w1 ? iv1 : iv0, w1 ? pw1 : pw0, c);
+                    carr2[b] = c;
                 }
             }
             __syncthreads();
-        }
-
-        // ---- load the block's rows (coalesced: kRowG contiguous values per column slot) ----
-        {
-            double2 tmp[G * C / T];
-#pragma unroll
-            for (int r = 0; r < G * C / T; ++r) {
-                const int qq = t + T * r, pos = qq / G, ra = qq % G;
-                tmp[r] = A.V[(size_t)pos * R + a0 + ra];
-            }
-#pragma unroll
-            for (int r = 0; r < G * C / T; ++r) {
-                const int qq = t + T * r, pos = qq / G, ra = qq % G;
-                bufs[ra * RS + phys(pos)] = tmp[r];
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int j = 0; j < E; ++j) v[j] = buf[phys(tr * E + j)];
-        inverse_from<GC, GC::P - 1, false>(v, buf, qtw, tr, gsync);
-        __syncthreads();  // the exchange buffers become the carry arrays
-
-        // ---- carry. Hop 1: unweight, round, round-off, two-digit chain per (row, column) from
-        //      zero: its carry-out goes to the next row. Hop 2: the incoming carry is folded into
-        //      the row's two digits; what leaves the second digit (a few units) goes to the next
-        //      row's first digit (hop 3, not renormalized). Carry-outs of hops 1 and 2 do not
-        //      depend on the previous block, so a block publishes both before waiting. ----
-        const double ia0 = __ldg(A.iwA + 2 * a), ia1 = __ldg(A.iwA + 2 * a + 1);
-#pragma unroll
-        for (int i = 0; i < E; ++i) {
-            const int b = tr + TR * i;
-            const int sb = __ldg(A.sB + b);
-            const double iwb = __ldg(A.iwB + b);
-            const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
-            const int s0 = o0 ? sA0 + sb - N : sA0 + sb, s1 = o1 ? sA1 + sb - N : sA1 + sb;
-            const double va = v[i].x * (ia0 * iwb) * (o0 ? 2.0 : 1.0);
-            const double vb = v[i].y * (ia1 * iwb) * (o1 ? 2.0 : 1.0);
-            long long la, lb, c;
-            const double ra = round_shift(va, la), rb = round_shift(vb, lb);
-            lerr = fmax(lerr, fmax(fabs(va - ra), fabs(vb - rb)));
-            const long long x0 = balance(la, A.q + (s0 < A.rem), c);
-            const long long x1 = balance(lb + c, A.q + (s1 < A.rem), c);
-            x0s[i] = (int)x0;
-            x1s[i] = (int)x1;
-            carr[rg * C + b] = c;
-            if (rg == G - 1) A.carry[(size_t)blk * C + b] = c;
-        }
-        atomicMax(&s_err, (unsigned long long)__double_as_longlong(lerr));
-        __syncthreads();
-        // hop 2 for rows fed from inside the block
-        if (rg > 0) {
+            // ---- hop 3: the small second-digit carry of the previous row into this row's first digit
 #pragma unroll
             for (int i = 0; i < E; ++i) {
                 const int b = tr + TR * i;
-                const int sb = __ldg(A.sB + b);
-                const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
-                const int s0 = o0 ? sA0 + sb - N : sA0 + sb, s1 = o1 ? sA1 + sb - N : sA1 + sb;
-                long long c;
-                x0s[i] = (int)balance((long long)x0s[i] + carr[(rg - 1) * C + b], A.q + (s0 < A.rem), c);
-                x1s[i] = (int)balance((long long)x1s[i] + c, A.q + (s1 < A.rem), c);
-                carr2[rg * C + b] = (int)c;
-                if (rg == G - 1) A.carry2[(size_t)blk * C + b] = (int)c;
+                double c2;
+                if (rg > 0)
+                    c2 = carr2[(rg - 1) * C + b];
+                else if (blk > 0)
+                    c2 = (double)__ldcg(A.carry2 + (size_t)(blk - 1) * C + b);
+                else
+                    c2 = hin2[b];
+                x0s[i] += c2;
             }
-        }
-        __threadfence();  // each writer orders its carry-out stores before the flag below
-        __syncthreads();
-        if (t == 0) {
-            __threadfence();
-            *reinterpret_cast<volatile unsigned*>(&A.ctl->flags[blk]) = ep + 1u;
-            if (blk > 0) wait_flag(&A.ctl->flags[blk - 1], ep + 1u, A.ctl, kSpinLimit);  // block blk-1's carries
-        }
-        __syncthreads();
-        // hop 2 for the block's first row: previous block's last row, or the wrap
-        if (rg == 0) {
+            if (MODE == LARGE_FINAL || A.dump) {
 #pragma unroll
-            for (int i = 0; i < E; ++i) {
-                const int b = tr + TR * i;
-                long long cin = (blk > 0) ? __ldcg(A.carry + (size_t)(blk - 1) * C + b) : hin[b];
-                if (a == 0 && b == 0) cin -= 2;  // the "- 2" of s^2 - 2 (digit 0)
-                const int sb = __ldg(A.sB + b);
-                const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
-                const int s0 = o0 ? sA0 + sb - N : sA0 + sb, s1 = o1 ? sA1 + sb - N : sA1 + sb;
-                long long c;
-                x0s[i] = (int)balance((long long)x0s[i] + cin, A.q + (s0 < A.rem), c);
-                x1s[i] = (int)balance((long long)x1s[i] + c, A.q + (s1 < A.rem), c);
-                carr2[b] = (int)c;
+                for (int i = 0; i < E; ++i) {
+                    const int b = tr + TR * i;
+                    const size_t m = (size_t)a + (size_t)R * b;
+                    *reinterpret_cast<int2*>(A.digits + 2 * m) =
+                        make_int2(__double2int_rn(x0s[i]), __double2int_rn(x1s[i]));
+                }
             }
-        }
-        __syncthreads();
-        // hop 3: the small second-digit carry of the previous row into this row's first digit
-#pragma unroll
-        for (int i = 0; i < E; ++i) {
-            const int b = tr + TR * i;
-            int c2;
-            if (rg > 0)
-                c2 = carr2[(rg - 1) * C + b];
-            else if (blk > 0)
-                c2 = __ldcg(A.carry2 + (size_t)(blk - 1) * C + b);
-            else
-                c2 = hin2[b];
-            x0s[i] += c2;
-        }
-        if (MODE == LARGE_FINAL || A.dump) {
-#pragma unroll
-            for (int i = 0; i < E; ++i) {
-                const int b = tr + TR * i;
-                const size_t m = (size_t)a + (size_t)R * b;
-                *reinterpret_cast<int2*>(A.digits + 2 * m) = make_int2(x0s[i], x1s[i]);
+            if (t == 0) {
+                const unsigned long long eb = s_err;
+                atomicMax(&A.ctl->err_max, eb);
+                atomicMax(&A.ctl->err_since, eb);
+                if (A.errlog) atomicMax(reinterpret_cast<unsigned int*>(A.errlog + (ep % (unsigned)A.errlog_len)),
+                                        __float_as_uint((float)__longlong_as_double((long long)eb)));
             }
-        }
-        if (t == 0) {
-            const unsigned long long eb = s_err;
-            atomicMax(&A.ctl->err_max, eb);
-            atomicMax(&A.ctl->err_since, eb);
-            if (A.errlog) atomicMax(reinterpret_cast<unsigned int*>(A.errlog + (ep % (unsigned)A.errlog_len)),
-                                    __float_as_uint((float)__longlong_as_double((long long)eb)));
         }
         if constexpr (MODE == LARGE_FINAL) return;
         __syncthreads();  // carry array reads done before the exchange buffers are reused
     }
 
-    // ---- weight, forward row FFT, twiddle, store ----
+    // ---- weight, forward row FFT, store ----
+    const int sA0 = __ldg(A.sA + 2 * a), sA1 = __ldg(A.sA + 2 * a + 1);
     const double wa0 = __ldg(A.wA + 2 * a), wa1 = __ldg(A.wA + 2 * a + 1);
 #pragma unroll
     for (int i = 0; i < E; ++i) {
@@ -302,14 +279,14 @@ __global__ void __launch_bounds__(kRowG * (1 << LOG_C) / (1 << kLargeLogE), 2) l
         const int sb = __ldg(A.sB + b);
         const double wb = __ldg(A.wB + b);
         const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
-        v[i].x = i2d_shift(x0s[i]) * (wa0 * wb) * (o0 ? 0.5 : 1.0);
-        v[i].y = i2d_shift(x1s[i]) * (wa1 * wb) * (o1 ? 0.5 : 1.0);
+        v[i].x = x0s[i] * (wa0 * wb) * (o0 ? 0.5 : 1.0);
+        v[i].y = x1s[i] * (wa1 * wb) * (o1 ? 0.5 : 1.0);
     }
     forward_from<GC, 0>(v, buf, qtw, tr, gsync);
 #pragma unroll
     for (int j = 0; j < E; ++j) buf[phys(tr * E + j)] = v[j];
     if (MODE == LARGE_ITER && blk == A.nblocks - 1 && t == 0) {
-        // rows R-2 and R-1 are block 0's wrap-around input: wait (bounded) until it has read them
+        // rows R-G .. R-1 are block 0's wrap-around input: wait (bounded) until it has read them
         wait_flag(&A.ctl->halo_read, ep + 1u, A.ctl, kSpinLimit);
     }
     __syncthreads();
@@ -324,7 +301,7 @@ __global__ void __launch_bounds__(kRowG * (1 << LOG_C) / (1 << kLargeLogE), 2) l
 // real-FFT split reads the partner column's spectrum from the other half's exchange buffer.
 // Block 0 holds column 0 and block C/2 column C/2, each of which pairs with itself.
 template <int LOG_R>
-__global__ void __launch_bounds__(2 * (1 << LOG_R) / (1 << kLargeLogE), 1) large_col(const LargeArgs A) {
+__global__ void __launch_bounds__(2 * (1 << LOG_R) / (1 << kLargeLogE), (LOG_R <= 11 ? 2 : 1)) large_col(const LargeArgs A) {
     using GR = SmallG<LOG_R, kLargeLogE>;
     constexpr int R = GR::M, TC = GR::T, E = GR::E;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -386,9 +363,8 @@ __global__ void __launch_bounds__(2 * (1 << LOG_R) / (1 << kLargeLogE), 1) large
 
 template <int LOG_C>
 static size_t row_smem() {
-    using GC = SmallGeom<LOG_C, kLargeLogE>;
-    return sizeof(double2) * kRowG * (GC::PAD + 1) + sizeof(double2) * qpad_len(GC::M / 4) +
-           2 * sizeof(long long) * GC::M + sizeof(int) * GC::M;
+    using GC = SmallG<LOG_C, kLargeLogE, TW_FULL>;
+    return sizeof(double2) * (large_rows_per_block(LOG_C) * (GC::PAD + 1) + twiddle_table_len<GC>());
 }
 
 template <int LOG_R>
@@ -411,7 +387,8 @@ static cudaError_t col_attr() {
 
 template <int LOG_C, int MODE>
 static cudaError_t row_t(const LargeArgs& a, cudaStream_t st) {
-    large_row<LOG_C, MODE><<<a.nblocks, kRowG * (1 << LOG_C) / (1 << kLargeLogE), row_smem<LOG_C>(), st>>>(a);
+    large_row<LOG_C, MODE>
+        <<<a.nblocks, large_rows_per_block(LOG_C) * (1 << LOG_C) / (1 << kLargeLogE), row_smem<LOG_C>(), st>>>(a);
     return cudaGetLastError();
 }
 
@@ -431,6 +408,7 @@ cudaError_t configure_large(int log_c, int log_r) {
         case 8: if (!(e = row_attr<8, LARGE_INIT>()) && !(e = row_attr<8, LARGE_ITER>())) e = row_attr<8, LARGE_FINAL>(); break;
         case 9: if (!(e = row_attr<9, LARGE_INIT>()) && !(e = row_attr<9, LARGE_ITER>())) e = row_attr<9, LARGE_FINAL>(); break;
         case 10: if (!(e = row_attr<10, LARGE_INIT>()) && !(e = row_attr<10, LARGE_ITER>())) e = row_attr<10, LARGE_FINAL>(); break;
+        case 11: if (!(e = row_attr<11, LARGE_INIT>()) && !(e = row_attr<11, LARGE_ITER>())) e = row_attr<11, LARGE_FINAL>(); break;
         default: return cudaErrorInvalidValue;
     }
     if (e) return e;
@@ -453,6 +431,7 @@ static cudaError_t row_mode(int log_c, const LargeArgs& a, cudaStream_t st) {
         case 8: return row_t<8, MODE>(a, st);
         case 9: return row_t<9, MODE>(a, st);
         case 10: return row_t<10, MODE>(a, st);
+        case 11: return row_t<11, MODE>(a, st);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -69,6 +69,14 @@ std::vector<double2> padded_quarter_table(uint64_t L) {
     return t;
 }
 
+// Every e^{-2 pi i r / L}, r < L, at slot qpad(r) (the row FFT's table: no quadrant fold).
+std::vector<double2> padded_full_table(uint64_t L) {
+    const uint64_t n = qpad_len((uint32_t)L);
+    std::vector<double2> t(n);
+    for (uint64_t i = 0; i < n; ++i) t[i] = padded_quarter_slot(L, i);
+    return t;
+}
+
 namespace {
 
 template <class T>
@@ -82,28 +90,45 @@ cudaError_t upload(T** d, const std::vector<T>& h) {
 
 bool large_length_supported(int log_n) { return log_n >= 14 && log_n <= 23; }
 
+// Row length (2^log_c complex values) of the two-pass FP64 engine at N = 2^log_n by default.
+int large_default_log_c(int log_n) {
+    return (log_n <= 15) ? log_n - 8 : (log_n <= 17) ? 8 : (log_n <= 19) ? 9 : 10;
+}
+
+// Splits of M = N/2 = 2^log_c rows x 2^(log_n - 1 - log_c) columns that the kernels implement:
+// rows of 2^6 .. 2^11, columns of 2^7 .. 2^12, at most kLargeMaxBlocks row blocks.
+bool large_split_supported(int log_n, int log_c) {
+    const int log_r = log_n - 1 - log_c;
+    if (!large_length_supported(log_n) || log_c < 6 || log_c > 11 || log_r < 7 || log_r > 12) return false;
+    return (1 << log_r) / large_rows_per_block(log_c) <= kLargeMaxBlocks;
+}
+
 LargeTest::~LargeTest() {
     if (exec) cudaGraphExecDestroy(exec);
-    void* ptrs[] = {V, carry, carry2, ctl, digits, errlog, qtwC, qtwR, tw1, tw2, pos_of_c, wA, iwA, sA, wB, iwB, sB};
+    void* ptrs[] = {V, carry, carry2, halo, ctl, digits, errlog, qtwC, qtwR, tw1, tw2, pos_of_c, wA, iwA, sA, wB, iwB, sB};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
 
-cudaError_t LargeTest::init(uint64_t p_, int log_n) {
+cudaError_t LargeTest::init(uint64_t p_, int log_n, int log_c) {
     p = p_;
     logN = log_n;
     const uint64_t N = 1ull << logN;
     M = N / 2;
-    logC = (logN <= 15) ? logN - 8 : (logN <= 17) ? 8 : (logN <= 19) ? 9 : 10;
+    logC = large_default_log_c(logN);
+    if (log_c >= 0) {
+        if (!large_split_supported(logN, log_c)) return cudaErrorInvalidValue;
+        logC = log_c;
+    }
     logR = logN - 1 - logC;
     C = 1 << logC;
     R = 1 << logR;
-    nblocks = R / kRowG;
+    nblocks = R / large_rows_per_block(logC);
     const int s = std::max(logC, (int)((logN - 1 + 1) / 2));
     cudaError_t e;
     if ((e = configure_large(logC, logR))) return e;
     // tables
-    if ((e = upload(&qtwC, padded_quarter_table(C)))) return e;
+    if ((e = upload(&qtwC, padded_full_table(C)))) return e;
     if ((e = upload(&qtwR, padded_quarter_table(R)))) return e;
     if ((e = upload(&tw1, omega_table(M, 1ull << s, 1)))) return e;
     if ((e = upload(&tw2, omega_table(M, M >> s, 1ull << s)))) return e;
@@ -133,8 +158,9 @@ cudaError_t LargeTest::init(uint64_t p_, int log_n) {
     if ((e = upload(&sB, hsB))) return e;
     // state
     if ((e = cudaMalloc(&V, M * sizeof(double2)))) return e;
-    if ((e = cudaMalloc(&carry, (size_t)nblocks * C * sizeof(long long)))) return e;
-    if ((e = cudaMalloc(&carry2, (size_t)nblocks * C * sizeof(int)))) return e;
+    if ((e = cudaMalloc(&carry, (size_t)nblocks * C * sizeof(double)))) return e;
+    if ((e = cudaMalloc(&carry2, (size_t)nblocks * C * sizeof(float)))) return e;
+    if ((e = cudaMalloc(&halo, (size_t)C * 2 * sizeof(double)))) return e;
     if ((e = cudaMalloc(&ctl, sizeof(LargeCtl)))) return e;
     if ((e = cudaMemset(ctl, 0, sizeof(LargeCtl)))) return e;
     if ((e = cudaMalloc(&digits, N * sizeof(int)))) return e;
@@ -158,6 +184,7 @@ cudaError_t LargeTest::init(uint64_t p_, int log_n) {
     A.sB = sB;
     A.carry = carry;
     A.carry2 = carry2;
+    A.halo = halo;
     A.ctl = ctl;
     A.digits = digits;
     A.errlog = errlog;

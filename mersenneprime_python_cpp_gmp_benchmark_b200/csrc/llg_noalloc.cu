@@ -54,21 +54,22 @@ constexpr size_t kStageBytes = 64u * 1024u;
 alignas(64) unsigned char g_stage[kStageBytes];
 
 struct Layout {
-    size_t V, carry, carry2, ctl, qtwC, qtwR, tw1, tw2, pos_of_c, wA, iwA, sA, wB, iwB, sB, end;
+    size_t V, carry, carry2, halo, ctl, qtwC, qtwR, tw1, tw2, pos_of_c, wA, iwA, sA, wB, iwB, sB, end;
 };
 
 size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 Layout layout(int logN, int logC, int logR, int s) {
     const size_t M = (size_t)1 << (logN - 1), C = (size_t)1 << logC, R = (size_t)1 << logR;
-    const size_t nblocks = R / kRowG;
+    const size_t nblocks = R / large_rows_per_block(logC);
     Layout L;
     size_t o = 0;
     L.V = o; o = up256(o + M * sizeof(double2));
-    L.carry = o; o = up256(o + nblocks * C * sizeof(long long));
-    L.carry2 = o; o = up256(o + nblocks * C * sizeof(int));
+    L.carry = o; o = up256(o + nblocks * C * sizeof(double));
+    L.carry2 = o; o = up256(o + nblocks * C * sizeof(float));
+    L.halo = o; o = up256(o + C * 2 * sizeof(double));
     L.ctl = o; o = up256(o + sizeof(LargeCtl));
-    L.qtwC = o; o = up256(o + qpad_len((uint32_t)(C / 4)) * sizeof(double2));
+    L.qtwC = o; o = up256(o + qpad_len((uint32_t)C) * sizeof(double2));
     L.qtwR = o; o = up256(o + qpad_len((uint32_t)(R / 4)) * sizeof(double2));
     L.tw1 = o; o = up256(o + ((size_t)1 << s) * sizeof(double2));
     L.tw2 = o; o = up256(o + (M >> s) * sizeof(double2));
@@ -172,7 +173,7 @@ extern "C" int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* 
         e = put_table<T>(base, off, cnt, [&](size_t i) -> T { return expr; }, st);      \
         if (e != cudaSuccess) return LLG_E_CUDA;                                        \
     } while (0)
-    PUT(double2, L.qtwC, (size_t)qpad_len((uint32_t)C / 4), padded_quarter_slot(C, i));
+    PUT(double2, L.qtwC, (size_t)qpad_len((uint32_t)C), padded_quarter_slot(C, i));
     PUT(double2, L.qtwR, (size_t)qpad_len((uint32_t)R / 4), padded_quarter_slot(R, i));
     PUT(double2, L.tw1, (size_t)1 << s, omega(M, i));
     PUT(double2, L.tw2, (size_t)(M >> s), omega(M, (uint64_t)i << s));
@@ -201,8 +202,9 @@ extern "C" int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* 
     A.wB = reinterpret_cast<const double*>(base + L.wB);
     A.iwB = reinterpret_cast<const double*>(base + L.iwB);
     A.sB = reinterpret_cast<const int*>(base + L.sB);
-    A.carry = reinterpret_cast<long long*>(base + L.carry);
-    A.carry2 = reinterpret_cast<int*>(base + L.carry2);
+    A.carry = reinterpret_cast<double*>(base + L.carry);
+    A.carry2 = reinterpret_cast<float*>(base + L.carry2);
+    A.halo = reinterpret_cast<double*>(base + L.halo);
     A.ctl = reinterpret_cast<LargeCtl*>(base + L.ctl);
     A.digits = digits_out;
     A.errlog = nullptr;
@@ -211,7 +213,7 @@ extern "C" int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* 
     A.tw_shift = s;
     A.C = C;
     A.R = R;
-    A.nblocks = R / kRowG;
+    A.nblocks = R / large_rows_per_block(logC);
     A.q = (int)(p >> logN);
     A.rem = (int)(p & (N - 1));
     A.logN = logN;

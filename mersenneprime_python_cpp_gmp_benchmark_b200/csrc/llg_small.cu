@@ -38,16 +38,16 @@ __global__ void __launch_bounds__(SmallGeom<LOG_M>::T, (SmallGeom<LOG_M>::T < 32
     ll_small_fp64(const SmallJob* __restrict__ jobs, const double2* __restrict__ qtw_g,
                   int64_t* __restrict__ digits_out, SmallResult* __restrict__ results,
                   float* __restrict__ errlog, double abort_err) {
-    using G = SmallG<LOG_M>;
+    using G = SmallG<LOG_M, 4, TW_QUARTER>;
     constexpr int M = G::M, N = G::N, E = G::E, T = G::T, W = G::W;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2* buf = reinterpret_cast<double2*>(smem_raw);          // exchange buffer, PAD slots
-    double2* qtw = buf + G::PAD;                                   // padded quarter table
-    constexpr int QL = (int)qpad_len(M / 4);
+    double2* qtw = buf + G::PAD;                                   // padded quarter-wave table
+    constexpr int QL = (int)twiddle_table_len<G>();
     double* wB = reinterpret_cast<double*>(qtw + QL);
     double* iwB = wB + E;
     int* sB = reinterpret_cast<int*>(iwB + E);
-    long long* cbuf = reinterpret_cast<long long*>(sB + E + (E & 1 ? 1 : 0) + 2);  // W * E
+    double* cbuf = reinterpret_cast<double*>(sB + E + (E & 1 ? 1 : 0) + 2);  // W * E
     unsigned long long* serr = reinterpret_cast<unsigned long long*>(cbuf + W * E);  // 2
 
     const int t = threadIdx.x;  // blockDim.x == T (a partial warp when T < 32)
@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(SmallGeom<LOG_M>::T, (SmallGeom<LOG_M>::T < 32
                 const double2 s = cadd(A, Bc), d = csub(A, Bc);
                 const double2 a3 = make_double2(3.0 * A.x - Bc.x, 3.0 * A.y - Bc.y);
                 const double2 d2 = make_double2((d.x - d.y) * (d.x + d.y), 2.0 * d.x * d.y);
-                const double2 w = twiddle<LOG_M>(qtw, (uint32_t)k, false);
+                const double2 w = twiddle_g<G>(qtw, (uint32_t)k, false);
                 v[j] = csub(cmul(a3, s), cmul(w, d2));
             }
             // the first inverse pass stores only after a barrier (partners may still be reading)
@@ -142,20 +142,20 @@ __global__ void __launch_bounds__(SmallGeom<LOG_M>::T, (SmallGeom<LOG_M>::T < 32
                 long long la, lb;
                 const double ra = round_shift(a, la), rb = round_shift(b, lb);
                 lerr = fmax(lerr, fmax(fabs(a - ra), fabs(b - rb)));
-                const int b0 = q + (s0 < rem), b1 = q + (s1 < rem);
-                long long c;
-                long long x0 = balance(la, b0, c);
-                const long long x1 = balance(lb + c, b1, c);
-                const long long cout = c;
+                const int b0 = q + (s0 < rem), b1 = q + (s1 < rem);  // digit sizes
+                double c;
+                double x0 = dsplit_e(ra, b0, c);
+                const double x1 = dsplit_e(rb + c, b1, c);
+                const double cout = c;
                 if (lane == lastlane) cbuf[warp * E + i] = cout;
-                const long long cin = __shfl_up_sync(wmask, cout, 1);
+                const double cin = __shfl_up_sync(wmask, cout, 1);
                 if (lane != 0) {
-                    x0 = balance(x0 + cin, b0, c);
-                    x1s[i] = (int)(x1 + c);
+                    x0 = dsplit_e(x0 + cin, b0, c);
+                    x1s[i] = d2i_exact(x1 + c);
                 } else {
-                    x1s[i] = (int)x1;
+                    x1s[i] = d2i_exact(x1);
                 }
-                x0s[i] = (int)x0;
+                x0s[i] = d2i_exact(x0);
             }
         }
         maxerr = fmax(maxerr, lerr);
@@ -168,17 +168,15 @@ __global__ void __launch_bounds__(SmallGeom<LOG_M>::T, (SmallGeom<LOG_M>::T < 32
         if (active && lane == 0) {
 #pragma unroll
             for (int i = 0; i < E; ++i) {
-                long long cin = (warp > 0) ? cbuf[(warp - 1) * E + i]
-                                           : cbuf[(W - 1) * E + ((i + E - 1) % E)];  // m-1 wraps at m=0
-                if (t == 0 && i == 0) cin -= 2;  // the "- 2" of s^2 - 2
+                double cin = (warp > 0) ? cbuf[(warp - 1) * E + i]
+                                        : cbuf[(W - 1) * E + ((i + E - 1) % E)];  // m-1 wraps at m=0
+                if (t == 0 && i == 0) cin -= 2.0;  // the "- 2" of s^2 - 2
                 const int sb = sB[i];
                 const bool o0 = sA0 + sb >= N;
                 const int s0 = o0 ? sA0 + sb - N : sA0 + sb;
-                const int b0 = q + (s0 < rem);
-                long long c;
-                const long long x0 = balance((long long)x0s[i] + cin, b0, c);
-                x0s[i] = (int)x0;
-                x1s[i] = (int)((long long)x1s[i] + c);
+                double c;
+                x0s[i] = d2i_exact(dsplit_e((double)x0s[i] + cin, q + (s0 < rem), c));
+                x1s[i] += (int)c;
             }
         }
         ++it;
@@ -325,11 +323,11 @@ cudaError_t launch_word(const SmallJob* jobs, int njobs, uint64_t* res, cudaStre
 
 template <int LOG_M>
 static size_t small_smem_bytes() {
-    using G = SmallGeom<LOG_M>;
+    using G = SmallG<LOG_M, 4, TW_QUARTER>;
     size_t b = sizeof(double2) * G::PAD;
-    b += sizeof(double2) * qpad_len(G::M / 4);
+    b += sizeof(double2) * twiddle_table_len<G>();
     b += 2 * sizeof(double) * G::E + sizeof(int) * (G::E + (G::E & 1 ? 1 : 0) + 2);
-    b += sizeof(long long) * G::W * G::E + 2 * sizeof(unsigned long long);
+    b += sizeof(double) * G::W * G::E + 2 * sizeof(unsigned long long);
     return b;
 }
 

@@ -74,6 +74,8 @@ def lib() -> ctypes.CDLL:
         L.llg_test_iterate.argtypes = [ctypes.c_void_p, u64, ctypes.c_void_p]
         L.llg_test_read.argtypes = [ctypes.c_void_p, ctypes.c_void_p, P(LlgResult), P(u64), sz]
         L.llg_test_errlog.argtypes = [ctypes.c_void_p, P(ctypes.c_float), sz, P(sz)]
+        L.llg_set_large_split.argtypes = [ctypes.c_int, ctypes.c_int]
+        L.llg_get_large_split.argtypes = [ctypes.c_int]
         L.llg_test_time_passes.argtypes = [ctypes.c_void_p, u64, ctypes.c_void_p, P(ctypes.c_double),
                                            P(ctypes.c_double)]
         L.llg_test_destroy.argtypes = [ctypes.c_void_p]
@@ -118,6 +120,23 @@ def fft_length(p, max_bpw=0.0):
 
 def ntt_length(p):
     return int(lib().llg_ntt_length(p))
+
+
+def set_large_split(log_n, log_c):
+    """Rows of 2^log_c complex values for the two-pass FP64 engine at N = 2^log_n (-1: default)."""
+    _check(lib().llg_set_large_split(log_n, log_c))
+
+
+def get_large_split(log_n):
+    return lib().llg_get_large_split(log_n)
+
+
+def large_splits(log_n):
+    """Row lengths (log2) the two-pass FP64 kernels implement at N = 2^log_n."""
+    old = get_large_split(log_n)
+    ok = [c for c in range(6, 12) if lib().llg_set_large_split(log_n, c) == 0]
+    set_large_split(log_n, old)
+    return ok
 
 
 def run(p, iters=0, engine="fp64", n=0, want_words=False):

@@ -205,3 +205,34 @@ def test_config_p1257787_full_run_trace(gpu, engine):
         log = t.errlog(65536)
         assert len(log) == 65536 and 0.0 < max(log) <= r["max_err"] + 1e-7
     t.close()
+
+
+@pytest.mark.parametrize("logn", [18, 20, 21, 22, 23])
+def test_every_split_full_residue(gpu, oracle, logn):
+    """Every row x column split the two-pass FP64 kernels implement at this length (the
+    autotuner's choices) gives the exact residue."""
+    n = 1 << logn
+    p = _odd_candidate(int(16.5 * n))
+    k = p.bit_length() + 4
+    want = oracle.ll_gmp(p, k)[2]
+    splits = gpu.large_splits(logn)
+    assert len(splits) >= 1
+    try:
+        for c in splits:
+            gpu.set_large_split(logn, c)
+            assert gpu.get_large_split(logn) == c
+            r = gpu.run(p, iters=k, n=n, want_words=True)
+            assert r["status"] == 0 and r["words"] == want, (logn, c)
+    finally:
+        gpu.set_large_split(logn, -1)
+
+
+def test_splits_p136279841_res64(gpu):
+    after = _after()
+    try:
+        for c in gpu.large_splits(23):
+            gpu.set_large_split(23, c)
+            r = gpu.run(136279841, iters=1000, n=1 << 23)
+            assert r["res64"] == after[(136279841, 1000)], c
+    finally:
+        gpu.set_large_split(23, -1)
