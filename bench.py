@@ -239,6 +239,12 @@ def bench_big(args, rank, world):
     import torch
     from mersenneprime_python_cpp_gmp_benchmark_b200 import llgpu
     n = 1 << 23
+    tuned = None
+    if args.engine == "fp64":
+        # the autotuner picks the row x column split of the two-pass engine on this GPU
+        best, cand = llgpu.autotune([23], save=False)[23]
+        tuned = {"rows": f"2^{best} complex", "columns": f"2^{22 - best} complex",
+                 "candidates_us": {f"2^{c}x2^{22 - c}": round(v, 2) for c, v in cand.items()}}
     stream = torch.cuda.Stream()
     handle = stream.cuda_stream
     t = llgpu.Test(BIG_P, n, args.engine)
@@ -302,11 +308,11 @@ def bench_big(args, rank, world):
         "dtype": "f64" if args.engine == "fp64" else "u64 (GF(2^64-2^32+1))",
         "data": "synthetic: the LL sequence of p=136,279,841 from s_0=4 (no external data)",
         "config": {"workload": ("p=136,279,841 FP64 IBDWT, N=2^23 (16.25 bits/digit), two-pass "
-                                "(row 1024 x column 4096 complex), 1000 squarings per step")
+                                "(rows x columns of 2^22 complex, split autotuned), 1000 squarings per step")
                    if args.engine == "fp64" else
                    ("p=136,279,841 Goldilocks NTT IBDWT, N=2^23 (16.25 bits/digit), two-pass "
                     "(row 1024 x column 8192), 1000 squarings per step"),
-                   "engine": args.engine,
+                   "engine": args.engine, "autotuned_split": tuned,
                    "l2": "flushed (512 MiB write) between steps; the 64 MiB state stays on device",
                    "parallelism": f"one independent test per GPU ({world} replica(s))"},
         "e2e": {"value": round(1e6 * t_e2e / k_e2e, 3), "unit": "us/iteration", "iters": k_e2e,

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <atomic>
 #include <map>
@@ -98,6 +99,8 @@ bool ntt_constants(int log_n, uint64_t& omega, NttConst& K) {
 }
 std::map<int, DeviceTables> g_tables;  // per device ordinal
 
+void load_tuning_once(int dev);
+
 int device_ready(int* dev_out) {
     int n = 0;
     cudaError_t e = cudaGetDeviceCount(&n);
@@ -107,6 +110,7 @@ int device_ready(int* dev_out) {
                     e != cudaSuccess ? cudaGetErrorString(e) : "device count 0");
     }
     CK(cudaGetDevice(dev_out));
+    load_tuning_once(*dev_out);
     return LLG_OK;
 }
 
@@ -421,6 +425,40 @@ struct SplitInit {
 } g_split_init;
 
 cudaError_t init_large(LargeTest& T, uint64_t p, int l) { return T.init(p, l, g_large_log_c[l].load()); }
+
+// The autotuner's choices (llgpu.autotune) persist in a text file, one line per choice:
+//   large_split <TAB> device name <TAB> log2 N <TAB> log2 row length
+// read once per process from $LLG_TUNE_CACHE, else $HOME/.cache/llgpu/tune.txt. Lines for other
+// devices or unsupported splits are ignored; llg_set_large_split overrides.
+void load_tuning_once(int dev) {
+    static std::once_flag once;
+    std::call_once(once, [dev] {
+        std::string path;
+        if (const char* e = std::getenv("LLG_TUNE_CACHE")) path = e;
+        else if (const char* h = std::getenv("HOME")) path = std::string(h) + "/.cache/llgpu/tune.txt";
+        if (path.empty()) return;
+        FILE* f = std::fopen(path.c_str(), "r");
+        if (!f) return;
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+            std::fclose(f);
+            return;
+        }
+        char line[512];
+        while (std::fgets(line, sizeof line, f)) {
+            char* fields[4] = {};
+            int nf = 0;
+            char* save = nullptr;
+            for (char* tok = strtok_r(line, "\t\n", &save); tok && nf < 4; tok = strtok_r(nullptr, "\t\n", &save))
+                fields[nf++] = tok;
+            if (nf != 4 || std::strcmp(fields[0], "large_split") != 0 || std::strcmp(fields[1], prop.name) != 0)
+                continue;
+            const int ln = std::atoi(fields[2]), lc = std::atoi(fields[3]);
+            if (large_split_supported(ln, lc)) g_large_log_c[ln].store(lc);
+        }
+        std::fclose(f);
+    });
+}
 cudaError_t init_large(NttLargeTest& T, uint64_t p, int l) { return T.init(p, l); }
 
 template <class TestT>

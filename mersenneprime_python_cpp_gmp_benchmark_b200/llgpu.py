@@ -139,6 +139,58 @@ def large_splits(log_n):
     return ok
 
 
+def tune_cache_path():
+    """Where the autotuner's choices live ($LLG_TUNE_CACHE, else ~/.cache/llgpu/tune.txt); the
+    library reads the file once per process, on its first device call."""
+    return os.environ.get("LLG_TUNE_CACHE") or os.path.join(os.path.expanduser("~"), ".cache", "llgpu",
+                                                             "tune.txt")
+
+
+def autotune(log_ns=range(14, 24), iters=64, warmup=16, save=True, path=None):
+    """Times every row x column split of the two-pass FP64 engine at each length N = 2^log_n on this
+    GPU (one exponent at ~16.5 bits/digit, `iters` squarings pass by pass after `warmup`), keeps
+    the fastest in force (llg_set_large_split) and, with `save`, records it in the tune file for
+    later processes. Returns {log_n: (best_log_c, {log_c: us per squaring})}."""
+    name = device_info()[0]
+    out = {}
+    for ln in log_ns:
+        n = 1 << ln
+        p = int(16.5 * n) | 1
+        times = {}
+        for c in large_splits(ln):
+            set_large_split(ln, c)
+            t = Test(p, n)
+            try:
+                t.start()
+                t.iterate(warmup)
+                r, k = t.time_passes(iters)
+                times[c] = r + k
+            finally:
+                t.close()
+        best = min(times, key=times.get)
+        set_large_split(ln, best)
+        out[ln] = (best, times)
+    if save:
+        path = path or tune_cache_path()
+        keep = []
+        if os.path.exists(path):
+            with open(path) as f:
+                for line in f:
+                    fl = line.rstrip("\n").split("\t")
+                    if len(fl) == 4 and fl[0] == "large_split" and fl[1] == name and int(fl[2]) in out:
+                        continue
+                    keep.append(line.rstrip("\n"))
+        os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
+        tmp = path + ".tmp"
+        with open(tmp, "w") as f:
+            for line in keep:
+                f.write(line + "\n")
+            for ln, (best, _) in sorted(out.items()):
+                f.write(f"large_split\t{name}\t{ln}\t{best}\n")
+        os.replace(tmp, path)
+    return out
+
+
 def run(p, iters=0, engine="fp64", n=0, want_words=False):
     """One test (or its first `iters` squarings) -> dict of llg_result fields (+ 'words')."""
     r = LlgResult()

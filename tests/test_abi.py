@@ -113,3 +113,32 @@ def test_mersenne_digits_formula_matches_string():
     sys.set_int_max_str_digits(0)
     for p in (3999, 4000, 4001, 4253, 9689, 21701, 44497, 86243):
         assert ll.mersenne_digits(p) == len(str(2**p - 1)), p
+
+
+def test_tune_file_round_trip(tmp_path, monkeypatch):
+    """The autotuner's file format: lines for other devices and lengths are kept, this device's
+    lengths are replaced (host-side logic only; the timing itself needs a GPU)."""
+    from mersenneprime_python_cpp_gmp_benchmark_b200 import llgpu
+    path = tmp_path / "tune.txt"
+    path.write_text("large_split\tOther GPU\t23\t11\nlarge_split\tNVIDIA B200\t22\t9\n")
+    monkeypatch.setenv("LLG_TUNE_CACHE", str(path))
+    assert llgpu.tune_cache_path() == str(path)
+    monkeypatch.setattr(llgpu, "device_info", lambda: ("NVIDIA B200", 148, 0))
+    monkeypatch.setattr(llgpu, "large_splits", lambda ln: [10, 11])
+    monkeypatch.setattr(llgpu, "set_large_split", lambda ln, c: None)
+
+    class FakeTest:
+        def __init__(self, p, n, engine="fp64"):
+            self.n = n
+        def start(self): pass
+        def iterate(self, k): pass
+        def time_passes(self, k):
+            return (100.0, 90.0)
+        def close(self): pass
+    monkeypatch.setattr(llgpu, "Test", FakeTest)
+    out = llgpu.autotune([22, 23], iters=4, warmup=1)
+    assert set(out) == {22, 23} and out[23][0] in (10, 11)
+    lines = path.read_text().splitlines()
+    assert "large_split\tOther GPU\t23\t11" in lines
+    assert sum(1 for l in lines if l.startswith("large_split\tNVIDIA B200\t22\t")) == 1
+    assert sum(1 for l in lines if l.startswith("large_split\tNVIDIA B200\t23\t")) == 1
