@@ -60,7 +60,7 @@ constexpr int kSmallLogMax = 13;  // N = 8192
 // ---- device tables ------------------------------------------------------------------------
 
 struct DeviceTables {
-    double2* qtw[kSmallLogMax + 1] = {};   // quarter-wave twiddles of the M = N/2 point FFT
+    std::map<uint32_t, double2*> qtw;      // quarter-wave twiddles of the M-point FFT, by M
     uint64_t* nqtw[kSmallLogMax + 1] = {}; // NTT: padded quarter table of the N-point transform
     NttConst nk[kSmallLogMax + 1] = {};
 };
@@ -114,21 +114,16 @@ int device_ready(int* dev_out) {
     return LLG_OK;
 }
 
-// e^{-2 pi i r / M}, r < M/4, rounded once from long double, stored at qpad(r) (the whole-test
-// kernel's quarter-wave table).
-std::vector<double2> quarter_table(int log_m) { return padded_quarter_table((uint64_t)1 << log_m); }
-
-int get_qtw(int dev, int log_m, const double2** out) {
+int get_qtw(int dev, uint32_t m, const double2** out) {
     std::lock_guard<std::mutex> lk(g_mx);
     DeviceTables& T = g_tables[dev];
-    if (!T.qtw[log_m]) {
-        std::vector<double2> h = quarter_table(log_m);  // padded layout (qpad)
-        double2* d = nullptr;
+    double2*& d = T.qtw[m];
+    if (!d) {
+        std::vector<double2> h = padded_quarter_table(m);  // padded layout (qpad)
         CK(cudaMalloc(&d, h.size() * sizeof(double2)));
         CK(cudaMemcpy(d, h.data(), h.size() * sizeof(double2), cudaMemcpyHostToDevice));
-        T.qtw[log_m] = d;
     }
-    *out = T.qtw[log_m];
+    *out = d;
     return LLG_OK;
 }
 
@@ -174,27 +169,49 @@ constexpr uint64_t kWordMaxP = 256;     // p below this runs on the exact multi-
 // base) and few enough for int32 digits and FP64 products.
 constexpr int kLargeLogMax = 23;
 
-bool is_small_length(uint64_t n) {
+bool is_small_pow2_length(uint64_t n) {
     const int l = ilog2_exact(n);
     return l >= kSmallLogMin && l <= kSmallLogMax;
+}
+
+// lengths of the whole-test kernels: 2^5 .. 2^13 and 3 x 2^10, 5 x 2^10, 3 x 2^11, 5 x 2^11, 3 x 2^12
+bool is_small_length(uint64_t n) {
+    return is_small_pow2_length(n) || (n < (1ull << 32) && mixed_length_supported((uint32_t)n, nullptr, nullptr));
+}
+
+int ceil_log2(uint64_t n) {
+    int l = 0;
+    while ((1ull << l) < n) ++l;
+    return l;
+}
+
+// every FP64 length, ascending
+const std::vector<uint32_t>& fp64_lengths() {
+    static const std::vector<uint32_t> v = [] {
+        std::vector<uint32_t> a;
+        for (int l = kSmallLogMin; l <= kLargeLogMax; ++l) a.push_back(1u << l);
+        for (uint32_t n = 1024; n <= (1u << 14); ++n)
+            if (mixed_length_supported(n, nullptr, nullptr)) a.push_back(n);
+        std::sort(a.begin(), a.end());
+        return a;
+    }();
+    return v;
 }
 
 // The two-pass engine's three-hop carry keeps digits balanced down to ~log2(N)/4 + 1 bits per
 // digit; it asks for floor(p/N) >= log2(N)/4 + 3.
 bool fp64_length_usable(uint64_t p, uint64_t n) {
+    if (n == 0 || (p + n - 1) / n > kMaxDigitBits) return false;
+    if (is_small_length(n)) return 2 * (p / n) >= (uint64_t)ceil_log2(n) + 4;
     const int l = ilog2_exact(n);
-    if ((p + n - 1) / n > kMaxDigitBits) return false;
-    if (is_small_length(n)) return 2 * (p / n) >= (uint64_t)l + 4;
     if (l > kSmallLogMax && large_length_supported(l)) return 4 * (p / n) >= (uint64_t)l + 12;
     return false;
 }
 
 // smallest usable length with p / N <= bpw
 uint32_t fp64_length(uint64_t p, double bpw) {
-    for (int l = kSmallLogMin; l <= kLargeLogMax; ++l) {
-        const uint64_t N = 1ull << l;
-        if ((double)p / (double)N <= bpw && fp64_length_usable(p, N)) return (uint32_t)N;
-    }
+    for (uint32_t N : fp64_lengths())
+        if ((double)p / (double)N <= bpw && fp64_length_usable(p, N)) return N;
     return 0;
 }
 
@@ -217,10 +234,8 @@ uint32_t ntt_len(uint64_t p) {
 }
 
 uint32_t next_fp64_length(uint64_t p, uint32_t n) {
-    for (int l = kSmallLogMin; l <= kLargeLogMax; ++l) {
-        const uint64_t N = 1ull << l;
-        if (N > n && fp64_length_usable(p, N)) return (uint32_t)N;
-    }
+    for (uint32_t N : fp64_lengths())
+        if (N > n && fp64_length_usable(p, N)) return N;
     return 0;
 }
 
@@ -327,13 +342,23 @@ int launch_group(llg_batch* b, Group& g, cudaStream_t caller) {
         if (rc) return rc;
         CK(launch_small_ntt(ilog2_exact(g.n), (const SmallJob*)g.d_jobs, cnt, qtw, K, (int64_t*)g.d_digits,
                             (SmallResult*)g.d_results, g.st));
-    } else {
+    } else if (is_small_pow2_length(g.n)) {
         const double2* qtw = nullptr;
-        int rc = get_qtw(b->dev, ilog2_exact(g.n) - 1, &qtw);
+        int rc = get_qtw(b->dev, g.n / 2, &qtw);
         if (rc) return rc;
         float* elog = (cnt == 1) ? b->d_errlog : nullptr;
         CK(launch_small_fp64(ilog2_exact(g.n), (const SmallJob*)g.d_jobs, cnt, qtw, (int64_t*)g.d_digits,
                              (SmallResult*)g.d_results, elog, kAbortErr, g.st));
+    } else {
+        int r0 = 0, ll = 0;
+        mixed_length_supported(g.n, &r0, &ll);
+        const double2 *qtwL = nullptr, *qtwM = nullptr;
+        int rc = get_qtw(b->dev, 1u << ll, &qtwL);
+        if (!rc) rc = get_qtw(b->dev, g.n / 2, &qtwM);
+        if (rc) return rc;
+        float* elog = (cnt == 1) ? b->d_errlog : nullptr;
+        CK(launch_small_fp64_mixed(g.n, (const SmallJob*)g.d_jobs, cnt, qtwL, qtwM, (int64_t*)g.d_digits,
+                                   (SmallResult*)g.d_results, elog, kAbortErr, g.st));
     }
     CK(cudaEventRecord(g.done, g.st));
     CK(cudaStreamWaitEvent(caller, g.done, 0));
@@ -589,7 +614,7 @@ int make_batch(const uint64_t* ps, size_t count, uint64_t max_iters, int engine,
             }
             it.n = n;
         }
-        if (it.n > (1u << kSmallLogMax))
+        if (it.n && !is_small_length(it.n))
             b->large.push_back(it);
         else
             groups[it.n].push_back(it);
@@ -598,9 +623,6 @@ int make_batch(const uint64_t* ps, size_t count, uint64_t max_iters, int engine,
         Group g;
         g.n = kv.first;
         g.items = std::move(kv.second);
-        // longest tests first: blocks start in index order, so the last wave holds the short ones
-        std::stable_sort(g.items.begin(), g.items.end(),
-                         [](const Item& x, const Item& y) { return x.iters > y.iters; });
         b->groups.push_back(std::move(g));
     }
     // largest lengths first (they run longest)
@@ -655,7 +677,7 @@ int collect_batch(llg_batch* b) {
     for (int round = 0; !retry.empty() && round < 16; ++round) {
         std::map<uint32_t, std::vector<Item>> byn;
         for (Item& it : retry) {
-            if (it.n > (1u << kSmallLogMax))
+            if (it.n && !is_small_length(it.n))
                 large.push_back(it);
             else
                 byn[it.n].push_back(it);

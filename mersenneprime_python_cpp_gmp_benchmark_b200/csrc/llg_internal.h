@@ -30,6 +30,13 @@ cudaError_t launch_small_fp64(int log_n, const SmallJob* jobs, int njobs, const 
                               int64_t* digits, SmallResult* results, float* errlog,
                               double abort_err, cudaStream_t st);
 
+// FP64 whole-test kernel for N = 2 R0 2^l (R0 = 3: l = 9..11; R0 = 5: l = 9..10); qtwL / qtwM:
+// padded quarter tables of 2^l and N/2 points.
+bool mixed_length_supported(uint32_t n, int* r0, int* log_l);
+cudaError_t launch_small_fp64_mixed(uint32_t n, const SmallJob* jobs, int njobs, const double2* qtwL,
+                                    const double2* qtwM, int64_t* digits, SmallResult* results,
+                                    float* errlog, double abort_err, cudaStream_t st);
+
 // p < 256: exact multi-limb word arithmetic, one thread per exponent (4 limbs out per exponent).
 cudaError_t launch_word(const SmallJob* jobs, int njobs, uint64_t* res, cudaStream_t st);
 

@@ -65,13 +65,21 @@ def test_fft_length_rules():
     from mersenneprime_python_cpp_gmp_benchmark_b200 import llgpu
     assert llgpu.fft_length(63) == 0 and llgpu.fft_length(255) == 0  # exact word kernel below 256
     prev = 0
-    for p in (256, 300, 521, 4423, 9689, 20011, 44497, 100001, 147456):
+
+    def kind(n):  # n = m 2^k with m in {1, 3, 5}, as the reference's lengths (lucaslehmer.cpp:244-254)
+        while n % 2 == 0:
+            n //= 2
+        return n
+    for p in (256, 300, 521, 4423, 9689, 20011, 44497, 60013, 80021, 100001, 147456):
         n = llgpu.fft_length(p)
-        assert n >= prev and n & (n - 1) == 0
+        assert n >= prev and kind(n) in (1, 3, 5)
         assert p / n <= 18.0 and p >= 2 * n
         prev = n
-    assert llgpu.fft_length(147457) == 0 or llgpu.fft_length(147457) > 8192
-    assert llgpu.fft_length(100001, 19.0) == 8192
+    # the non-power-of-two whole-test lengths
+    assert llgpu.fft_length(44497) == 3072 and llgpu.fft_length(80021) == 5120
+    assert llgpu.fft_length(100001) == 6144 and llgpu.fft_length(150001) == 10240
+    assert llgpu.fft_length(200001) == 12288 and llgpu.fft_length(250001) == 16384
+    assert llgpu.fft_length(100001, 19.0) == 6144
 
 
 def test_run_without_gpu_fails_loudly():

@@ -128,3 +128,38 @@ def test_ntt_interim_residue(gpu, oracle):
     for p, k in ((4423, 3), (86243, 1000), (204791, 77)):
         r = gpu.run(p, iters=k, engine="ntt", want_words=True)
         assert r["words"] == oracle.ll_gmp(p, k)[2]
+
+
+# ---- the non-power-of-two whole-test lengths (3 x 2^k, 5 x 2^k) --------------------------------
+
+@pytest.mark.parametrize("n", [3072, 5120, 6144, 10240, 12288])
+def test_mixed_length_full_residue(gpu, oracle, n):
+    """Every {3,5} x 2^k length, exponents from the bits-per-digit floor to 18 bits per digit,
+    full residues (every limb) after all p - 2 squarings or an interim k."""
+    rng = random.Random(n)
+    lo = n * ((n.bit_length() + 4 + 1) // 2)
+    ps = [p for p in oracle.primes(lo, min(18 * n, 230000)) if p % 2]
+    picks = sorted(rng.sample(ps, 3)) + [max(ps)]
+    for p in picks:
+        k = 0 if p < 60000 else 3000  # full tests where the oracle finishes in seconds
+        r = gpu.run(p, n=n, iters=k, want_words=True)
+        assert r["status"] == 0 and r["n"] == n, (p, n, r)
+        assert r["words"] == oracle.ll_gmp(p, k)[2], (p, n)
+        assert r["max_err"] < 0.4
+
+
+def test_mixed_lengths_in_batch(gpu, oracle):
+    """A batch mixing power-of-two and {3,5} x 2^k buckets, results in input order."""
+    ps = [44497, 40009, 80021, 9689, 99991, 86243, 150001, 4423]
+    rs = gpu.run_batch(ps, iters=2000, want_words=True)
+    lengths = {r["p"]: r["n"] for r in rs}
+    assert lengths[44497] == 3072 and lengths[80021] == 5120 and lengths[99991] == 6144
+    for p, r in zip(ps, rs):
+        assert r["p"] == p and r["words"] == oracle.ll_gmp(p, 2000)[2], p
+
+
+def test_mixed_length_known_primes(gpu):
+    """The Mersenne exponents whose lengths are 3 x 2^10 and 5 x 2^10 (full tests: residue zero)."""
+    for p in (44497, 86243):
+        r = gpu.run(p)
+        assert r["n"] in (3072, 5120) and r["is_zero"] == 1 and r["status"] == 0, r
