@@ -243,8 +243,9 @@ def bench_big(args, rank, world):
     if args.engine == "fp64":
         # the autotuner picks the row x column split of the two-pass engine on this GPU
         best, cand = llgpu.autotune([23], save=False)[23]
-        tuned = {"rows": f"2^{best} complex", "columns": f"2^{22 - best} complex",
-                 "candidates_us": {f"2^{c}x2^{22 - c}": round(v, 2) for c, v in cand.items()}}
+        tuned = {"row_length": f"2^{best[0]} complex", "column_length": f"2^{22 - best[0]} complex",
+                 "rows_per_block": best[1],
+                 "candidates_us": {f"2^{c}x2^{22 - c}/{g}": round(v, 2) for (c, g), v in cand.items()}}
     stream = torch.cuda.Stream()
     handle = stream.cuda_stream
     t = llgpu.Test(BIG_P, n, args.engine)

@@ -70,12 +70,14 @@ double llg_get_max_bpw(void);
  * Replaces ntt_length(), cuda/ll_ntt.cu:172-180. */
 uint32_t llg_ntt_length(uint64_t p);
 /* Shape of the two-pass FP64 engine at N = 2^log_n (2^14 .. 2^23): rows of 2^log_c complex
- * values, columns of 2^(log_n - 1 - log_c). Tests created afterwards use it; log_c < 0 restores
- * the built-in choice. The autotuner (llgpu.autotune) times the supported splits and sets the
- * fastest. No reference counterpart (FFTW_MEASURE planning, lucaslehmer.cpp:232-242, is the
- * nearest). llg_get_large_split returns the split in force (-1 for a length without one). */
-int llg_set_large_split(int log_n, int log_c);
-int llg_get_large_split(int log_n);
+ * values, columns of 2^(log_n - 1 - log_c), `rows` rows per row-pass block (2 or 4; 0: the
+ * default for log_c). Tests created afterwards use it; log_c < 0 restores the built-in shape. The
+ * autotuner (llgpu.autotune) times the supported shapes and sets the fastest. No reference
+ * counterpart (FFTW_MEASURE planning, lucaslehmer.cpp:232-242, is the nearest).
+ * llg_get_large_split returns the row length in force (-1 for a length without one) and its rows
+ * per block in *rows (may be null). */
+int llg_set_large_split(int log_n, int log_c, int rows);
+int llg_get_large_split(int log_n, int* rows);
 /* Largest exponent an engine handles. Replaces max_exponent(), cuda/ll_ntt.cu:279. */
 uint64_t llg_max_exponent(int engine);
 

@@ -440,19 +440,26 @@ double bits_to_double(unsigned long long b) {
     return d;
 }
 
-// Row length of the two-pass FP64 engine per log2 N (-1: the built-in default); set by
-// llg_set_large_split (the autotuner's choice).
-std::atomic<int> g_large_log_c[kLargeLogMax + 1];
+// Shape of the two-pass FP64 engine per log2 N: row length (log2) and rows per row-pass block
+// (-1 / 0: the built-in defaults); set by llg_set_large_split (the autotuner's choice). The two
+// are packed in one word so a reader never sees half of an update.
+std::atomic<int> g_large_shape[kLargeLogMax + 1];
 struct SplitInit {
     SplitInit() {
-        for (auto& x : g_large_log_c) x.store(-1);
+        for (auto& x : g_large_shape) x.store(-1);
     }
 } g_split_init;
 
-cudaError_t init_large(LargeTest& T, uint64_t p, int l) { return T.init(p, l, g_large_log_c[l].load()); }
+int shape_log_c(int v) { return v < 0 ? -1 : v & 0xff; }
+int shape_rows(int v) { return v < 0 ? 0 : v >> 8; }
+
+cudaError_t init_large(LargeTest& T, uint64_t p, int l) {
+    const int v = g_large_shape[l].load();
+    return T.init(p, l, shape_log_c(v), shape_rows(v));
+}
 
 // The autotuner's choices (llgpu.autotune) persist in a text file, one line per choice:
-//   large_split <TAB> device name <TAB> log2 N <TAB> log2 row length
+//   large_split <TAB> device name <TAB> log2 N <TAB> log2 row length <TAB> rows per block
 // read once per process from $LLG_TUNE_CACHE, else $HOME/.cache/llgpu/tune.txt. Lines for other
 // devices or unsupported splits are ignored; llg_set_large_split overrides.
 void load_tuning_once(int dev) {
@@ -471,15 +478,15 @@ void load_tuning_once(int dev) {
         }
         char line[512];
         while (std::fgets(line, sizeof line, f)) {
-            char* fields[4] = {};
+            char* fields[5] = {};
             int nf = 0;
             char* save = nullptr;
-            for (char* tok = strtok_r(line, "\t\n", &save); tok && nf < 4; tok = strtok_r(nullptr, "\t\n", &save))
+            for (char* tok = strtok_r(line, "\t\n", &save); tok && nf < 5; tok = strtok_r(nullptr, "\t\n", &save))
                 fields[nf++] = tok;
-            if (nf != 4 || std::strcmp(fields[0], "large_split") != 0 || std::strcmp(fields[1], prop.name) != 0)
+            if (nf != 5 || std::strcmp(fields[0], "large_split") != 0 || std::strcmp(fields[1], prop.name) != 0)
                 continue;
-            const int ln = std::atoi(fields[2]), lc = std::atoi(fields[3]);
-            if (large_split_supported(ln, lc)) g_large_log_c[ln].store(lc);
+            const int ln = std::atoi(fields[2]), lc = std::atoi(fields[3]), rows = std::atoi(fields[4]);
+            if (large_split_supported(ln, lc, rows)) g_large_shape[ln].store(lc | (rows << 8));
         }
         std::fclose(f);
     });
@@ -781,18 +788,24 @@ uint32_t llg_fft_length(uint64_t p, double max_bpw) {
     return fp64_length(p, max_bpw);
 }
 
-int llg_set_large_split(int log_n, int log_c) {
+int llg_set_large_split(int log_n, int log_c, int rows) {
     if (!large_length_supported(log_n)) return fail(LLG_E_ARG, "log2 N = %d is not a two-pass length", log_n);
-    if (log_c >= 0 && !large_split_supported(log_n, log_c))
-        return fail(LLG_E_UNSUPPORTED, "no kernels for rows of 2^%d at N = 2^%d", log_c, log_n);
-    g_large_log_c[log_n].store(log_c < 0 ? -1 : log_c);
+    if (log_c < 0) {
+        g_large_shape[log_n].store(-1);
+        return LLG_OK;
+    }
+    if (!large_split_supported(log_n, log_c, rows))
+        return fail(LLG_E_UNSUPPORTED, "no kernels for rows of 2^%d, %d per block, at N = 2^%d", log_c, rows, log_n);
+    g_large_shape[log_n].store(log_c | ((rows ? rows : large_rows_per_block(log_c)) << 8));
     return LLG_OK;
 }
 
-int llg_get_large_split(int log_n) {
+int llg_get_large_split(int log_n, int* rows) {
     if (!large_length_supported(log_n)) return -1;
-    const int v = g_large_log_c[log_n].load();
-    return v >= 0 ? v : large_default_log_c(log_n);
+    const int v = g_large_shape[log_n].load();
+    const int lc = v >= 0 ? shape_log_c(v) : large_default_log_c(log_n);
+    if (rows) *rows = v >= 0 ? shape_rows(v) : large_rows_per_block(lc);
+    return lc;
 }
 
 int llg_set_max_bpw(double b) {

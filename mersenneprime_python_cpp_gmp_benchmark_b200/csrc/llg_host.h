@@ -14,9 +14,9 @@ constexpr int kGraphChunk = 64;  // squarings per captured CUDA graph
 
 bool large_length_supported(int log_n);
 int large_default_log_c(int log_n);
-bool large_split_supported(int log_n, int log_c);
+bool large_split_supported(int log_n, int log_c, int rows);
 int set_error(int code, const char* msg);  // records this thread's llg_last_error() text
-cudaError_t configure_large(int log_c, int log_r);
+cudaError_t configure_large(int log_c, int g, int log_r);
 std::vector<int> seed_digits(uint64_t n);
 // Quarter-wave table of an L-point FFT in the padded layout the kernels read (entry r at qpad(r)).
 std::vector<double2> padded_quarter_table(uint64_t L);
@@ -25,12 +25,13 @@ double2 padded_quarter_slot(uint64_t L, uint64_t i);
 
 struct LargeTest {
     uint64_t p = 0, M = 0;
-    int logN = 0, logC = 0, logR = 0, C = 0, R = 0, nblocks = 0;
+    int logN = 0, logC = 0, logR = 0, C = 0, R = 0, rows = 0, nblocks = 0;
     double2* V = nullptr;
     double* carry = nullptr;
     float* carry2 = nullptr;
     double* halo = nullptr;
     LargeCtl* ctl = nullptr;
+    unsigned* flags = nullptr;
     int* digits = nullptr;
     float* errlog = nullptr;
     int errlog_len = 0;
@@ -43,7 +44,8 @@ struct LargeTest {
     uint64_t done = 0;  // squarings enqueued since start()
 
     ~LargeTest();
-    cudaError_t init(uint64_t p, int log_n, int log_c = -1);              // log_c < 0: default split
+    // log_c < 0: the default split; rows == 0: the default rows per row-pass block
+    cudaError_t init(uint64_t p, int log_n, int log_c = -1, int rows = 0);
     cudaError_t start(const std::vector<int>& digits, cudaStream_t st);  // INIT + first squaring
     cudaError_t step(uint64_t k, cudaStream_t st);                        // k more squarings
     cudaError_t step_plain(uint64_t k, bool dump_last, cudaStream_t st);

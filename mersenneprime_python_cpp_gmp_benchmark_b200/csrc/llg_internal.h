@@ -58,8 +58,11 @@ constexpr int kRowG = 4;              // rows per row-pass block (rows of up to 
 __host__ __device__
 #endif
 constexpr int large_rows_per_block(int log_c) { return log_c >= 11 ? 2 : kRowG; }
+// row-pass shapes with kernels: 4 rows per block for rows of 2^6 .. 2^10, 2 rows for 2^8 .. 2^11
+constexpr bool large_rows_supported(int log_c, int g) {
+    return (g == 4 && log_c >= 6 && log_c <= 10) || (g == 2 && log_c >= 8 && log_c <= 11);
+}
 constexpr int kLargeLogE = 4;         // log2 of the complex values per thread in the two-pass kernels
-constexpr int kLargeMaxBlocks = 1024; // row blocks (R / kRowG) supported by the control block
 
 struct LargeCtl {
     unsigned int epoch;              // squarings whose column pass has finished; +1 per column pass
@@ -68,7 +71,6 @@ struct LargeCtl {
     unsigned long long err_max;      // bits of the max round-off over the run (double, >= 0)
     unsigned long long err_since;    // same, since the host last cleared it
     unsigned int halo_read;          // epoch + 1 once block 0 has read the wrap-around rows
-    unsigned int flags[kLargeMaxBlocks];  // flags[k] = epoch + 1 once block k published its carries
 };
 
 enum { LARGE_INIT = 0, LARGE_ITER = 1, LARGE_FINAL = 2 };
@@ -108,6 +110,7 @@ struct LargeArgs {
     float* carry2;            // [nblocks][C] hop-2 carry-outs (integers of a few units)
     double* halo;             // [2][C] block 0's wrap-around carries (hop 2, hop 3)
     LargeCtl* ctl;
+    unsigned int* flags;      // [nblocks] epoch + 1 once block k published its carries
     int* digits;              // N int32, natural order (INIT input; dump / FINAL output)
     float* errlog;            // per-epoch max round-off ring (may be null)
     int errlog_len;
@@ -118,7 +121,7 @@ struct LargeArgs {
     int logN;
 };
 
-cudaError_t launch_large_row(int log_c, int mode, const LargeArgs& a, cudaStream_t st);
+cudaError_t launch_large_row(int log_c, int g, int mode, const LargeArgs& a, cudaStream_t st);
 cudaError_t launch_large_col(int log_r, const LargeArgs& a, cudaStream_t st);
 
 // ---- two-pass exact NTT engine (N = 2^14 .. 2^23): N field elements in HBM ------------------
@@ -141,6 +144,7 @@ struct NttLargeArgs {
     int* c3;                  // [nblocks][C] hop-3 carry-outs
     long long* halo;          // block 0's wrap-around carries: C int64 + 2 * C int32
     LargeCtl* ctl;
+    unsigned int* flags;      // [nblocks] epoch + 1 once block k published its carries
     int* digits;              // N int32, natural order (INIT input; dump / FINAL output)
     int dump;
     int tw_shift;

@@ -53,11 +53,13 @@ __device__ __forceinline__ double2 twiddle_M(const LargeArgs& A, uint32_t x, boo
 
 }  // namespace
 
-template <int LOG_C, int MODE>
-__global__ void __launch_bounds__(large_rows_per_block(LOG_C) * (1 << LOG_C) / (1 << kLargeLogE), 2)
+constexpr int large_row_threads(int log_c, int g) { return g * (1 << log_c) / (1 << kLargeLogE); }
+
+template <int LOG_C, int G, int MODE>
+__global__ void __launch_bounds__(large_row_threads(LOG_C, G), 512 / (large_row_threads(LOG_C, G) < 32 ? 32 : large_row_threads(LOG_C, G)))
     large_row(const LargeArgs A) {
     using GC = SmallG<LOG_C, kLargeLogE, TW_FULL>;  // full twiddle table
-    constexpr int C = GC::M, TR = GC::T, E = GC::E, G = large_rows_per_block(LOG_C), T = G * TR;
+    constexpr int C = GC::M, TR = GC::T, E = GC::E, T = G * TR;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int RS = GC::PAD + 1;  // row-buffer stride: odd, so the rows of a slot hit different banks
     constexpr int QL = (int)twiddle_table_len<GC>();
@@ -214,8 +216,8 @@ __global__ void __launch_bounds__(large_rows_per_block(LOG_C) * (1 << LOG_C) / (
             __syncthreads();
             if (t == 0) {
                 __threadfence();
-                *reinterpret_cast<volatile unsigned*>(&A.ctl->flags[blk]) = ep + 1u;
-                if (blk > 0) wait_flag(&A.ctl->flags[blk - 1], ep + 1u, A.ctl, kSpinLimit);  // block blk-1's carries
+                *reinterpret_cast<volatile unsigned*>(&A.flags[blk]) = ep + 1u;
+                if (blk > 0) wait_flag(&A.flags[blk - 1], ep + 1u, A.ctl, kSpinLimit);  // block blk-1's carries
             }
             __syncthreads();
             // ---- hop 2 for the block's first row: previous block's last row, or the wrap ----
@@ -361,10 +363,10 @@ __global__ void __launch_bounds__(2 * (1 << LOG_R) / (1 << kLargeLogE), (LOG_R <
     if (cb == 0 && t == 0) atomicAdd(&A.ctl->epoch, 1u);
 }
 
-template <int LOG_C>
+template <int LOG_C, int G>
 static size_t row_smem() {
     using GC = SmallG<LOG_C, kLargeLogE, TW_FULL>;
-    return sizeof(double2) * (large_rows_per_block(LOG_C) * (GC::PAD + 1) + twiddle_table_len<GC>());
+    return sizeof(double2) * (G * (GC::PAD + 1) + twiddle_table_len<GC>());
 }
 
 template <int LOG_R>
@@ -373,10 +375,18 @@ static size_t col_smem() {
     return sizeof(double2) * 2 * GR::PAD + sizeof(double2) * qpad_len(GR::M / 4) + sizeof(double2) * 2 * GR::E;
 }
 
-template <int LOG_C, int MODE>
+template <int LOG_C, int G, int MODE>
 static cudaError_t row_attr() {
-    return cudaFuncSetAttribute(large_row<LOG_C, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)row_smem<LOG_C>());
+    return cudaFuncSetAttribute(large_row<LOG_C, G, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)row_smem<LOG_C, G>());
+}
+
+template <int LOG_C, int G>
+static cudaError_t row_attrs() {
+    cudaError_t e = row_attr<LOG_C, G, LARGE_INIT>();
+    if (!e) e = row_attr<LOG_C, G, LARGE_ITER>();
+    if (!e) e = row_attr<LOG_C, G, LARGE_FINAL>();
+    return e;
 }
 
 template <int LOG_R>
@@ -385,10 +395,9 @@ static cudaError_t col_attr() {
                                 (int)col_smem<LOG_R>());
 }
 
-template <int LOG_C, int MODE>
+template <int LOG_C, int G, int MODE>
 static cudaError_t row_t(const LargeArgs& a, cudaStream_t st) {
-    large_row<LOG_C, MODE>
-        <<<a.nblocks, large_rows_per_block(LOG_C) * (1 << LOG_C) / (1 << kLargeLogE), row_smem<LOG_C>(), st>>>(a);
+    large_row<LOG_C, G, MODE><<<a.nblocks, G * (1 << LOG_C) / (1 << kLargeLogE), row_smem<LOG_C, G>(), st>>>(a);
     return cudaGetLastError();
 }
 
@@ -400,15 +409,20 @@ static cudaError_t col_t(const LargeArgs& a, cudaStream_t st) {
 
 // Opts the kernels of one geometry into their dynamic shared memory (once per device, before
 // any launch or graph capture).
-cudaError_t configure_large(int log_c, int log_r) {
+cudaError_t configure_large(int log_c, int g, int log_r) {
     cudaError_t e = cudaSuccess;
-    switch (log_c) {
-        case 6: if (!(e = row_attr<6, LARGE_INIT>()) && !(e = row_attr<6, LARGE_ITER>())) e = row_attr<6, LARGE_FINAL>(); break;
-        case 7: if (!(e = row_attr<7, LARGE_INIT>()) && !(e = row_attr<7, LARGE_ITER>())) e = row_attr<7, LARGE_FINAL>(); break;
-        case 8: if (!(e = row_attr<8, LARGE_INIT>()) && !(e = row_attr<8, LARGE_ITER>())) e = row_attr<8, LARGE_FINAL>(); break;
-        case 9: if (!(e = row_attr<9, LARGE_INIT>()) && !(e = row_attr<9, LARGE_ITER>())) e = row_attr<9, LARGE_FINAL>(); break;
-        case 10: if (!(e = row_attr<10, LARGE_INIT>()) && !(e = row_attr<10, LARGE_ITER>())) e = row_attr<10, LARGE_FINAL>(); break;
-        case 11: if (!(e = row_attr<11, LARGE_INIT>()) && !(e = row_attr<11, LARGE_ITER>())) e = row_attr<11, LARGE_FINAL>(); break;
+    if (!large_rows_supported(log_c, g)) return cudaErrorInvalidValue;
+    const int key = 16 * log_c + g;
+    switch (key) {
+        case 16 * 6 + 4: e = row_attrs<6, 4>(); break;
+        case 16 * 7 + 4: e = row_attrs<7, 4>(); break;
+        case 16 * 8 + 4: e = row_attrs<8, 4>(); break;
+        case 16 * 9 + 4: e = row_attrs<9, 4>(); break;
+        case 16 * 10 + 4: e = row_attrs<10, 4>(); break;
+        case 16 * 8 + 2: e = row_attrs<8, 2>(); break;
+        case 16 * 9 + 2: e = row_attrs<9, 2>(); break;
+        case 16 * 10 + 2: e = row_attrs<10, 2>(); break;
+        case 16 * 11 + 2: e = row_attrs<11, 2>(); break;
         default: return cudaErrorInvalidValue;
     }
     if (e) return e;
@@ -424,23 +438,26 @@ cudaError_t configure_large(int log_c, int log_r) {
 }
 
 template <int MODE>
-static cudaError_t row_mode(int log_c, const LargeArgs& a, cudaStream_t st) {
-    switch (log_c) {
-        case 6: return row_t<6, MODE>(a, st);
-        case 7: return row_t<7, MODE>(a, st);
-        case 8: return row_t<8, MODE>(a, st);
-        case 9: return row_t<9, MODE>(a, st);
-        case 10: return row_t<10, MODE>(a, st);
-        case 11: return row_t<11, MODE>(a, st);
+static cudaError_t row_mode(int log_c, int g, const LargeArgs& a, cudaStream_t st) {
+    switch (16 * log_c + g) {
+        case 16 * 6 + 4: return row_t<6, 4, MODE>(a, st);
+        case 16 * 7 + 4: return row_t<7, 4, MODE>(a, st);
+        case 16 * 8 + 4: return row_t<8, 4, MODE>(a, st);
+        case 16 * 9 + 4: return row_t<9, 4, MODE>(a, st);
+        case 16 * 10 + 4: return row_t<10, 4, MODE>(a, st);
+        case 16 * 8 + 2: return row_t<8, 2, MODE>(a, st);
+        case 16 * 9 + 2: return row_t<9, 2, MODE>(a, st);
+        case 16 * 10 + 2: return row_t<10, 2, MODE>(a, st);
+        case 16 * 11 + 2: return row_t<11, 2, MODE>(a, st);
         default: return cudaErrorInvalidValue;
     }
 }
 
-cudaError_t launch_large_row(int log_c, int mode, const LargeArgs& a, cudaStream_t st) {
+cudaError_t launch_large_row(int log_c, int g, int mode, const LargeArgs& a, cudaStream_t st) {
     switch (mode) {
-        case LARGE_INIT: return row_mode<LARGE_INIT>(log_c, a, st);
-        case LARGE_ITER: return row_mode<LARGE_ITER>(log_c, a, st);
-        case LARGE_FINAL: return row_mode<LARGE_FINAL>(log_c, a, st);
+        case LARGE_INIT: return row_mode<LARGE_INIT>(log_c, g, a, st);
+        case LARGE_ITER: return row_mode<LARGE_ITER>(log_c, g, a, st);
+        case LARGE_FINAL: return row_mode<LARGE_FINAL>(log_c, g, a, st);
         default: return cudaErrorInvalidValue;
     }
 }

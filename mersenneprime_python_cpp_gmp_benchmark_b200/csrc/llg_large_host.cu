@@ -95,38 +95,37 @@ int large_default_log_c(int log_n) {
     return (log_n <= 15) ? log_n - 8 : (log_n <= 17) ? 8 : (log_n <= 19) ? 9 : 10;
 }
 
-// Splits of M = N/2 = 2^log_c rows x 2^(log_n - 1 - log_c) columns that the kernels implement:
-// rows of 2^6 .. 2^11, columns of 2^7 .. 2^12, at most kLargeMaxBlocks row blocks.
-bool large_split_supported(int log_n, int log_c) {
+// Shapes of M = N/2 = 2^log_r rows of 2^log_c values (row blocks of `rows` rows) that the
+// kernels implement: rows of 2^6 .. 2^11, columns of 2^7 .. 2^12; rows == 0: the default.
+bool large_split_supported(int log_n, int log_c, int rows) {
     const int log_r = log_n - 1 - log_c;
-    if (!large_length_supported(log_n) || log_c < 6 || log_c > 11 || log_r < 7 || log_r > 12) return false;
-    return (1 << log_r) / large_rows_per_block(log_c) <= kLargeMaxBlocks;
+    if (rows == 0) rows = large_rows_per_block(log_c);
+    return large_length_supported(log_n) && log_r >= 7 && log_r <= 12 && large_rows_supported(log_c, rows);
 }
 
 LargeTest::~LargeTest() {
     if (exec) cudaGraphExecDestroy(exec);
-    void* ptrs[] = {V, carry, carry2, halo, ctl, digits, errlog, qtwC, qtwR, tw1, tw2, pos_of_c, wA, iwA, sA, wB, iwB, sB};
+    void* ptrs[] = {V, carry, carry2, halo, ctl, flags, digits, errlog, qtwC, qtwR, tw1, tw2, pos_of_c, wA, iwA, sA, wB, iwB, sB};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
 
-cudaError_t LargeTest::init(uint64_t p_, int log_n, int log_c) {
+cudaError_t LargeTest::init(uint64_t p_, int log_n, int log_c, int rows_) {
     p = p_;
     logN = log_n;
     const uint64_t N = 1ull << logN;
     M = N / 2;
     logC = large_default_log_c(logN);
-    if (log_c >= 0) {
-        if (!large_split_supported(logN, log_c)) return cudaErrorInvalidValue;
-        logC = log_c;
-    }
+    if (log_c >= 0) logC = log_c;
+    rows = rows_ ? rows_ : large_rows_per_block(logC);
+    if (!large_split_supported(logN, logC, rows)) return cudaErrorInvalidValue;
     logR = logN - 1 - logC;
     C = 1 << logC;
     R = 1 << logR;
-    nblocks = R / large_rows_per_block(logC);
+    nblocks = R / rows;
     const int s = std::max(logC, (int)((logN - 1 + 1) / 2));
     cudaError_t e;
-    if ((e = configure_large(logC, logR))) return e;
+    if ((e = configure_large(logC, rows, logR))) return e;
     // tables
     if ((e = upload(&qtwC, padded_full_table(C)))) return e;
     if ((e = upload(&qtwR, padded_quarter_table(R)))) return e;
@@ -163,6 +162,8 @@ cudaError_t LargeTest::init(uint64_t p_, int log_n, int log_c) {
     if ((e = cudaMalloc(&halo, (size_t)C * 2 * sizeof(double)))) return e;
     if ((e = cudaMalloc(&ctl, sizeof(LargeCtl)))) return e;
     if ((e = cudaMemset(ctl, 0, sizeof(LargeCtl)))) return e;
+    if ((e = cudaMalloc(&flags, (size_t)nblocks * sizeof(unsigned)))) return e;
+    if ((e = cudaMemset(flags, 0, (size_t)nblocks * sizeof(unsigned)))) return e;
     if ((e = cudaMalloc(&digits, N * sizeof(int)))) return e;
     errlog_len = 1 << 16;
     if ((e = cudaMalloc(&errlog, errlog_len * sizeof(float)))) return e;
@@ -186,6 +187,7 @@ cudaError_t LargeTest::init(uint64_t p_, int log_n, int log_c) {
     A.carry2 = carry2;
     A.halo = halo;
     A.ctl = ctl;
+    A.flags = flags;
     A.digits = digits;
     A.errlog = errlog;
     A.errlog_len = errlog_len;
@@ -204,8 +206,9 @@ cudaError_t LargeTest::start(const std::vector<int>& d, cudaStream_t st) {
     cudaError_t e;
     if ((e = cudaMemcpyAsync(digits, d.data(), d.size() * sizeof(int), cudaMemcpyHostToDevice, st))) return e;
     if ((e = cudaMemsetAsync(ctl, 0, sizeof(LargeCtl), st))) return e;
+    if ((e = cudaMemsetAsync(flags, 0, (size_t)nblocks * sizeof(unsigned), st))) return e;
     if ((e = cudaMemsetAsync(errlog, 0, errlog_len * sizeof(float), st))) return e;
-    if ((e = launch_large_row(logC, LARGE_INIT, args, st))) return e;
+    if ((e = launch_large_row(logC, rows, LARGE_INIT, args, st))) return e;
     if ((e = launch_large_col(logR, args, st))) return e;
     done = 1;
     return cudaSuccess;
@@ -216,7 +219,7 @@ cudaError_t LargeTest::step_plain(uint64_t k, bool dump_last, cudaStream_t st) {
     for (uint64_t i = 0; i < k; ++i) {
         LargeArgs a = args;
         a.dump = (dump_last && i + 1 == k) ? 1 : 0;
-        if ((e = launch_large_row(logC, LARGE_ITER, a, st))) return e;
+        if ((e = launch_large_row(logC, rows, LARGE_ITER, a, st))) return e;
         if ((e = launch_large_col(logR, a, st))) return e;
     }
     done += k;
@@ -231,7 +234,7 @@ cudaError_t LargeTest::step(uint64_t k, cudaStream_t st) {
         if ((e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking))) return e;
         if ((e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal))) return e;
         for (int i = 0; i < kGraphChunk; ++i) {
-            launch_large_row(logC, LARGE_ITER, args, cap);
+            launch_large_row(logC, rows, LARGE_ITER, args, cap);
             launch_large_col(logR, args, cap);
         }
         cudaGraph_t g;
@@ -253,16 +256,17 @@ cudaError_t LargeTest::step(uint64_t k, cudaStream_t st) {
 
 cudaError_t LargeTest::finish(cudaStream_t st, std::vector<int>& out) {
     cudaError_t e;
-    if ((e = launch_large_row(logC, LARGE_FINAL, args, st))) return e;
+    if ((e = launch_large_row(logC, rows, LARGE_FINAL, args, st))) return e;
     // the squarings may resume from this state at the same epoch: clear the flags FINAL set
-    if ((e = cudaMemsetAsync(&ctl->halo_read, 0, sizeof(LargeCtl) - offsetof(LargeCtl, halo_read), st))) return e;
+    if ((e = cudaMemsetAsync(&ctl->halo_read, 0, sizeof(unsigned), st))) return e;
+    if ((e = cudaMemsetAsync(flags, 0, (size_t)nblocks * sizeof(unsigned), st))) return e;
     out.resize(2 * M);
     if ((e = cudaMemcpyAsync(out.data(), digits, 2 * M * sizeof(int), cudaMemcpyDeviceToHost, st))) return e;
     return cudaStreamSynchronize(st);
 }
 
 cudaError_t LargeTest::read_ctl(LargeCtl& h, cudaStream_t st) {
-    cudaError_t e = cudaMemcpyAsync(&h, ctl, offsetof(LargeCtl, flags), cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaMemcpyAsync(&h, ctl, sizeof(LargeCtl), cudaMemcpyDeviceToHost, st);
     if (e) return e;
     return cudaStreamSynchronize(st);
 }
@@ -309,7 +313,7 @@ cudaError_t time_pairs(uint64_t k, cudaStream_t st, Row row, Col col, double& ro
 
 cudaError_t LargeTest::time_passes(uint64_t k, cudaStream_t st, double& row_us, double& col_us) {
     cudaError_t e = time_pairs(
-        k, st, [&] { return launch_large_row(logC, LARGE_ITER, args, st); },
+        k, st, [&] { return launch_large_row(logC, rows, LARGE_ITER, args, st); },
         [&] { return launch_large_col(logR, args, st); }, row_us, col_us);
     if (!e) done += k;
     return e;
@@ -460,13 +464,15 @@ cudaError_t NttLargeTest::init(uint64_t p_, int log_n) {
         (e = up(pc, &cpc)) || (e = up(hwA, &cwA)) || (e = up(hiwA, &ciwA)) || (e = up(hsA, &csA)) ||
         (e = up(hwB, &cwB)) || (e = up(hiwB, &ciwB)) || (e = up(hsB, &csB)))
         return e;
-    void *dV, *dc1, *dc2, *dc3, *dh, *dctl, *dd;
+    void *dV, *dc1, *dc2, *dc3, *dh, *dctl, *dd, *dfl;
     if ((e = alloc(N * sizeof(uint64_t), &dV)) || (e = alloc((size_t)nblocks * C * sizeof(long long), &dc1)) ||
         (e = alloc((size_t)nblocks * C * sizeof(int), &dc2)) || (e = alloc((size_t)nblocks * C * sizeof(int), &dc3)) ||
         (e = alloc((size_t)C * (sizeof(long long) + 2 * sizeof(int)), &dh)) ||
-        (e = alloc(sizeof(LargeCtl), &dctl)) || (e = alloc(N * sizeof(int), &dd)))
+        (e = alloc(sizeof(LargeCtl), &dctl)) || (e = alloc(N * sizeof(int), &dd)) ||
+        (e = alloc((size_t)nblocks * sizeof(unsigned), &dfl)))
         return e;
     if ((e = cudaMemset(dctl, 0, sizeof(LargeCtl)))) return e;
+    if ((e = cudaMemset(dfl, 0, (size_t)nblocks * sizeof(unsigned)))) return e;
     ctl = static_cast<LargeCtl*>(dctl);
     digits = static_cast<int*>(dd);
     A.V = static_cast<uint64_t*>(dV);
@@ -486,6 +492,7 @@ cudaError_t NttLargeTest::init(uint64_t p_, int log_n) {
     A.c3 = static_cast<int*>(dc3);
     A.halo = static_cast<long long*>(dh);
     A.ctl = ctl;
+    A.flags = static_cast<unsigned*>(dfl);
     A.digits = digits;
     A.dump = 0;
     A.tw_shift = s;
@@ -502,6 +509,7 @@ cudaError_t NttLargeTest::start(const std::vector<int>& d, cudaStream_t st) {
     cudaError_t e;
     if ((e = cudaMemcpyAsync(digits, d.data(), d.size() * sizeof(int), cudaMemcpyHostToDevice, st))) return e;
     if ((e = cudaMemsetAsync(ctl, 0, sizeof(LargeCtl), st))) return e;
+    if ((e = cudaMemsetAsync(args.flags, 0, (size_t)nblocks * sizeof(unsigned), st))) return e;
     if ((e = launch_ntt_row(logC, LARGE_INIT, args, st))) return e;
     if ((e = launch_ntt_col(logR, args, st))) return e;
     done = 1;
@@ -543,7 +551,8 @@ cudaError_t NttLargeTest::step(uint64_t k, cudaStream_t st) {
 cudaError_t NttLargeTest::finish(cudaStream_t st, std::vector<int>& out) {
     cudaError_t e;
     if ((e = launch_ntt_row(logC, LARGE_FINAL, args, st))) return e;
-    if ((e = cudaMemsetAsync(&ctl->halo_read, 0, sizeof(LargeCtl) - offsetof(LargeCtl, halo_read), st))) return e;
+    if ((e = cudaMemsetAsync(&ctl->halo_read, 0, sizeof(unsigned), st))) return e;
+    if ((e = cudaMemsetAsync(args.flags, 0, (size_t)nblocks * sizeof(unsigned), st))) return e;
     out.resize(N);
     if ((e = cudaMemcpyAsync(out.data(), digits, N * sizeof(int), cudaMemcpyDeviceToHost, st))) return e;
     return cudaStreamSynchronize(st);
@@ -558,7 +567,7 @@ cudaError_t NttLargeTest::time_passes(uint64_t k, cudaStream_t st, double& row_u
 }
 
 cudaError_t NttLargeTest::read_ctl(LargeCtl& h, cudaStream_t st) {
-    cudaError_t e = cudaMemcpyAsync(&h, ctl, offsetof(LargeCtl, flags), cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaMemcpyAsync(&h, ctl, sizeof(LargeCtl), cudaMemcpyDeviceToHost, st);
     if (e) return e;
     return cudaStreamSynchronize(st);
 }

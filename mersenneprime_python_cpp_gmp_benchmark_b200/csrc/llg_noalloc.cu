@@ -54,7 +54,7 @@ constexpr size_t kStageBytes = 64u * 1024u;
 alignas(64) unsigned char g_stage[kStageBytes];
 
 struct Layout {
-    size_t V, carry, carry2, halo, ctl, qtwC, qtwR, tw1, tw2, pos_of_c, wA, iwA, sA, wB, iwB, sB, end;
+    size_t V, carry, carry2, halo, ctl, flags, qtwC, qtwR, tw1, tw2, pos_of_c, wA, iwA, sA, wB, iwB, sB, end;
 };
 
 size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -69,6 +69,7 @@ Layout layout(int logN, int logC, int logR, int s) {
     L.carry2 = o; o = up256(o + nblocks * C * sizeof(float));
     L.halo = o; o = up256(o + C * 2 * sizeof(double));
     L.ctl = o; o = up256(o + sizeof(LargeCtl));
+    L.flags = o; o = up256(o + nblocks * sizeof(unsigned));
     L.qtwC = o; o = up256(o + qpad_len((uint32_t)C) * sizeof(double2));
     L.qtwR = o; o = up256(o + qpad_len((uint32_t)(R / 4)) * sizeof(double2));
     L.tw1 = o; o = up256(o + ((size_t)1 << s) * sizeof(double2));
@@ -163,7 +164,7 @@ extern "C" int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* 
     }
     unsigned char* base = g_scratch_addr[dev];
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    cudaError_t e = configure_large(logC, logR);
+    cudaError_t e = configure_large(logC, large_rows_per_block(logC), logR);
     if (e != cudaSuccess) return LLG_E_CUDA;
 
     // tables (exact integers and long-double rounded values, as the allocating path uses)
@@ -206,6 +207,7 @@ extern "C" int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* 
     A.carry2 = reinterpret_cast<float*>(base + L.carry2);
     A.halo = reinterpret_cast<double*>(base + L.halo);
     A.ctl = reinterpret_cast<LargeCtl*>(base + L.ctl);
+    A.flags = reinterpret_cast<unsigned*>(base + L.flags);
     A.digits = digits_out;
     A.errlog = nullptr;
     A.errlog_len = 1;
@@ -224,15 +226,16 @@ extern "C" int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* 
     if (cudaMemcpyAsync(digits_out, &four, sizeof four, cudaMemcpyHostToDevice, st) != cudaSuccess)
         return LLG_E_CUDA;
     if (cudaMemsetAsync(A.ctl, 0, sizeof(LargeCtl), st) != cudaSuccess) return LLG_E_CUDA;
-    if (launch_large_row(logC, LARGE_INIT, A, st) != cudaSuccess) return LLG_E_CUDA;
+    if (cudaMemsetAsync(A.flags, 0, (size_t)A.nblocks * sizeof(unsigned), st) != cudaSuccess) return LLG_E_CUDA;
+    if (launch_large_row(logC, large_rows_per_block(logC), LARGE_INIT, A, st) != cudaSuccess) return LLG_E_CUDA;
     if (launch_large_col(logR, A, st) != cudaSuccess) return LLG_E_CUDA;
     for (uint64_t k = 1; k < iters; ++k) {
-        if (launch_large_row(logC, LARGE_ITER, A, st) != cudaSuccess) return LLG_E_CUDA;
+        if (launch_large_row(logC, large_rows_per_block(logC), LARGE_ITER, A, st) != cudaSuccess) return LLG_E_CUDA;
         if (launch_large_col(logR, A, st) != cudaSuccess) return LLG_E_CUDA;
     }
-    if (launch_large_row(logC, LARGE_FINAL, A, st) != cudaSuccess) return LLG_E_CUDA;
+    if (launch_large_row(logC, large_rows_per_block(logC), LARGE_FINAL, A, st) != cudaSuccess) return LLG_E_CUDA;
     LargeCtl h;
-    if (cudaMemcpyAsync(&h, A.ctl, offsetof(LargeCtl, flags), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    if (cudaMemcpyAsync(&h, A.ctl, sizeof(LargeCtl), cudaMemcpyDeviceToHost, st) != cudaSuccess)
         return LLG_E_CUDA;
     if (cudaStreamSynchronize(st) != cudaSuccess) return LLG_E_CUDA;
     double err;

@@ -223,8 +223,8 @@ __global__ void __launch_bounds__(kNttRowG * (1 << LOG_C) / 16, 2) ntt_row(const
         __syncthreads();
         if (t == 0) {
             __threadfence();
-            *reinterpret_cast<volatile unsigned*>(&A.ctl->flags[blk]) = ep + 1u;
-            if (blk > 0) wait_flag(&A.ctl->flags[blk - 1], ep + 1u, A.ctl, kNttSpinLimit);
+            *reinterpret_cast<volatile unsigned*>(&A.flags[blk]) = ep + 1u;
+            if (blk > 0) wait_flag(&A.flags[blk - 1], ep + 1u, A.ctl, kNttSpinLimit);
         }
         __syncthreads();
         const long long* hin1 = A.halo;

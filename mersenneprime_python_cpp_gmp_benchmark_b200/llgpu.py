@@ -74,8 +74,8 @@ def lib() -> ctypes.CDLL:
         L.llg_test_iterate.argtypes = [ctypes.c_void_p, u64, ctypes.c_void_p]
         L.llg_test_read.argtypes = [ctypes.c_void_p, ctypes.c_void_p, P(LlgResult), P(u64), sz]
         L.llg_test_errlog.argtypes = [ctypes.c_void_p, P(ctypes.c_float), sz, P(sz)]
-        L.llg_set_large_split.argtypes = [ctypes.c_int, ctypes.c_int]
-        L.llg_get_large_split.argtypes = [ctypes.c_int]
+        L.llg_set_large_split.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.llg_get_large_split.argtypes = [ctypes.c_int, P(ctypes.c_int)]
         L.llg_test_time_passes.argtypes = [ctypes.c_void_p, u64, ctypes.c_void_p, P(ctypes.c_double),
                                            P(ctypes.c_double)]
         L.llg_test_destroy.argtypes = [ctypes.c_void_p]
@@ -122,20 +122,24 @@ def ntt_length(p):
     return int(lib().llg_ntt_length(p))
 
 
-def set_large_split(log_n, log_c):
-    """Rows of 2^log_c complex values for the two-pass FP64 engine at N = 2^log_n (-1: default)."""
-    _check(lib().llg_set_large_split(log_n, log_c))
+def set_large_split(log_n, log_c, rows=0):
+    """Shape of the two-pass FP64 engine at N = 2^log_n: rows of 2^log_c complex values, `rows` rows
+    per row-pass block (0: the default for log_c); log_c = -1 restores the built-in shape."""
+    _check(lib().llg_set_large_split(log_n, log_c, rows))
 
 
 def get_large_split(log_n):
-    return lib().llg_get_large_split(log_n)
+    """(log2 row length, rows per block) in force at N = 2^log_n."""
+    rows = ctypes.c_int()
+    lc = lib().llg_get_large_split(log_n, ctypes.byref(rows))
+    return lc, rows.value
 
 
 def large_splits(log_n):
-    """Row lengths (log2) the two-pass FP64 kernels implement at N = 2^log_n."""
+    """The (log2 row length, rows per block) shapes the two-pass FP64 kernels implement at 2^log_n."""
     old = get_large_split(log_n)
-    ok = [c for c in range(6, 12) if lib().llg_set_large_split(log_n, c) == 0]
-    set_large_split(log_n, old)
+    ok = [(c, g) for c in range(6, 12) for g in (4, 2) if lib().llg_set_large_split(log_n, c, g) == 0]
+    set_large_split(log_n, *old)
     return ok
 
 
@@ -147,10 +151,11 @@ def tune_cache_path():
 
 
 def autotune(log_ns=range(14, 24), iters=64, warmup=16, save=True, path=None):
-    """Times every row x column split of the two-pass FP64 engine at each length N = 2^log_n on this
-    GPU (one exponent at ~16.5 bits/digit, `iters` squarings pass by pass after `warmup`), keeps
-    the fastest in force (llg_set_large_split) and, with `save`, records it in the tune file for
-    later processes. Returns {log_n: (best_log_c, {log_c: us per squaring})}."""
+    """Times every shape (row x column split, rows per row-pass block) of the two-pass FP64 engine
+    at each length N = 2^log_n on this GPU (one exponent at ~16.5 bits/digit, `iters` squarings
+    pass by pass after `warmup`), keeps the fastest in force (llg_set_large_split) and, with
+    `save`, records it in the tune file for later processes.
+    Returns {log_n: ((log_c, rows), {(log_c, rows): us per squaring})}."""
     name = device_info()[0]
     out = {}
     for ln in log_ns:
@@ -158,7 +163,7 @@ def autotune(log_ns=range(14, 24), iters=64, warmup=16, save=True, path=None):
         p = int(16.5 * n) | 1
         times = {}
         for c in large_splits(ln):
-            set_large_split(ln, c)
+            set_large_split(ln, *c)
             t = Test(p, n)
             try:
                 t.start()
@@ -168,7 +173,7 @@ def autotune(log_ns=range(14, 24), iters=64, warmup=16, save=True, path=None):
             finally:
                 t.close()
         best = min(times, key=times.get)
-        set_large_split(ln, best)
+        set_large_split(ln, *best)
         out[ln] = (best, times)
     if save:
         path = path or tune_cache_path()
@@ -177,7 +182,7 @@ def autotune(log_ns=range(14, 24), iters=64, warmup=16, save=True, path=None):
             with open(path) as f:
                 for line in f:
                     fl = line.rstrip("\n").split("\t")
-                    if len(fl) == 4 and fl[0] == "large_split" and fl[1] == name and int(fl[2]) in out:
+                    if len(fl) >= 4 and fl[0] == "large_split" and fl[1] == name and int(fl[2]) in out:
                         continue
                     keep.append(line.rstrip("\n"))
         os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
@@ -186,7 +191,7 @@ def autotune(log_ns=range(14, 24), iters=64, warmup=16, save=True, path=None):
             for line in keep:
                 f.write(line + "\n")
             for ln, (best, _) in sorted(out.items()):
-                f.write(f"large_split\t{name}\t{ln}\t{best}\n")
+                f.write(f"large_split\t{name}\t{ln}\t{best[0]}\t{best[1]}\n")
         os.replace(tmp, path)
     return out
 

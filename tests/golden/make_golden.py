@@ -134,7 +134,9 @@ def range_(workers: int, hi: int = 100001):
         rng = random.Random(1)
         check += rng.sample([p for p in ps if p > 30001], 400)
         for p, v, r in pool.imap_unordered(_range_ref, sorted(check, reverse=True), chunksize=1):
-            assert rows[p][0] == v and rows[p][1] == r, f"oracle != reference at p={p}"
+            # p = 2 returns before any squaring (lucaslehmer.cpp:29), leaving the thread's previous
+            # res64 in place: only its verdict is defined
+            assert rows[p][0] == v and (p == 2 or rows[p][1] == r), f"oracle != reference at p={p}"
     with open(os.path.join(HERE, "range_100001.csv"), "w") as f:
         f.write("# p,is_prime,res64,residue_blake2b64 -- oracle GMP restatement; reference res64 "
                 f"checked on {len(check)} exponents\n")

@@ -128,12 +128,12 @@ def test_tune_file_round_trip(tmp_path, monkeypatch):
     lengths are replaced (host-side logic only; the timing itself needs a GPU)."""
     from mersenneprime_python_cpp_gmp_benchmark_b200 import llgpu
     path = tmp_path / "tune.txt"
-    path.write_text("large_split\tOther GPU\t23\t11\nlarge_split\tNVIDIA B200\t22\t9\n")
+    path.write_text("large_split\tOther GPU\t23\t11\t2\nlarge_split\tNVIDIA B200\t22\t9\t4\n")
     monkeypatch.setenv("LLG_TUNE_CACHE", str(path))
     assert llgpu.tune_cache_path() == str(path)
     monkeypatch.setattr(llgpu, "device_info", lambda: ("NVIDIA B200", 148, 0))
-    monkeypatch.setattr(llgpu, "large_splits", lambda ln: [10, 11])
-    monkeypatch.setattr(llgpu, "set_large_split", lambda ln, c: None)
+    monkeypatch.setattr(llgpu, "large_splits", lambda ln: [(10, 4), (10, 2), (11, 2)])
+    monkeypatch.setattr(llgpu, "set_large_split", lambda ln, c, g=0: None)
 
     class FakeTest:
         def __init__(self, p, n, engine="fp64"):
@@ -145,8 +145,8 @@ def test_tune_file_round_trip(tmp_path, monkeypatch):
         def close(self): pass
     monkeypatch.setattr(llgpu, "Test", FakeTest)
     out = llgpu.autotune([22, 23], iters=4, warmup=1)
-    assert set(out) == {22, 23} and out[23][0] in (10, 11)
+    assert set(out) == {22, 23} and out[23][0] in ((10, 4), (10, 2), (11, 2))
     lines = path.read_text().splitlines()
-    assert "large_split\tOther GPU\t23\t11" in lines
+    assert "large_split\tOther GPU\t23\t11\t2" in lines
     assert sum(1 for l in lines if l.startswith("large_split\tNVIDIA B200\t22\t")) == 1
     assert sum(1 for l in lines if l.startswith("large_split\tNVIDIA B200\t23\t")) == 1

@@ -219,7 +219,7 @@ def test_every_split_full_residue(gpu, oracle, logn):
     assert len(splits) >= 1
     try:
         for c in splits:
-            gpu.set_large_split(logn, c)
+            gpu.set_large_split(logn, *c)
             assert gpu.get_large_split(logn) == c
             r = gpu.run(p, iters=k, n=n, want_words=True)
             assert r["status"] == 0 and r["words"] == want, (logn, c)
@@ -231,7 +231,7 @@ def test_splits_p136279841_res64(gpu):
     after = _after()
     try:
         for c in gpu.large_splits(23):
-            gpu.set_large_split(23, c)
+            gpu.set_large_split(23, *c)
             r = gpu.run(136279841, iters=1000, n=1 << 23)
             assert r["res64"] == after[(136279841, 1000)], c
     finally:
