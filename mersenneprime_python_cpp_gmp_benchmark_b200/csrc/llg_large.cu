@@ -423,6 +423,8 @@ cudaError_t configure_large(int log_c, int g, int log_r) {
         case 16 * 9 + 2: e = row_attrs<9, 2>(); break;
         case 16 * 10 + 2: e = row_attrs<10, 2>(); break;
         case 16 * 11 + 2: e = row_attrs<11, 2>(); break;
+        case 16 * 9 + 8: e = row_attrs<9, 8>(); break;
+        case 16 * 10 + 8: e = row_attrs<10, 8>(); break;
         default: return cudaErrorInvalidValue;
     }
     if (e) return e;
@@ -449,6 +451,8 @@ static cudaError_t row_mode(int log_c, int g, const LargeArgs& a, cudaStream_t s
         case 16 * 9 + 2: return row_t<9, 2, MODE>(a, st);
         case 16 * 10 + 2: return row_t<10, 2, MODE>(a, st);
         case 16 * 11 + 2: return row_t<11, 2, MODE>(a, st);
+        case 16 * 9 + 8: return row_t<9, 8, MODE>(a, st);
+        case 16 * 10 + 8: return row_t<10, 8, MODE>(a, st);
         default: return cudaErrorInvalidValue;
     }
 }

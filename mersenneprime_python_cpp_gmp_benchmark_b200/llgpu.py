@@ -138,7 +138,7 @@ def get_large_split(log_n):
 def large_splits(log_n):
     """The (log2 row length, rows per block) shapes the two-pass FP64 kernels implement at 2^log_n."""
     old = get_large_split(log_n)
-    ok = [(c, g) for c in range(6, 12) for g in (4, 2) if lib().llg_set_large_split(log_n, c, g) == 0]
+    ok = [(c, g) for c in range(6, 12) for g in (4, 2, 8) if lib().llg_set_large_split(log_n, c, g) == 0]
     set_large_split(log_n, *old)
     return ok
 

@@ -163,3 +163,21 @@ def test_mixed_length_known_primes(gpu):
     for p in (44497, 86243):
         r = gpu.run(p)
         assert r["n"] in (3072, 5120) and r["is_zero"] == 1 and r["status"] == 0, r
+
+
+def test_all_primes_to_100001_full_residues(gpu, oracle):
+    """Config: every prime p <= 100001 (9592 exponents, 28 hits) in one batch, the mix of lengths
+    the engine picks (power-of-two and {3,5} x 2^k): every full residue's fingerprint equals the
+    oracle's (tests/golden/range_100001.csv), and the hit set is the known list."""
+    from conftest import known_exponents
+    rows = load_range()
+    ps = oracle.primes(2, 100001)
+    out = gpu.run_batch(ps, want_words=True)
+    hits = []
+    for p, r in zip(ps, out):
+        v, res, h = rows[p]
+        assert r["status"] == 0, p
+        assert (bool(r["is_zero"]), r["res64"], oracle.residue_hash(r["words"])) == (v, res, h), p
+        if r["is_zero"]:
+            hits.append(p)
+    assert hits == [p for p in known_exponents() if p <= 100001]
