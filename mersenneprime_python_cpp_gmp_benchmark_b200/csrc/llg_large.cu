@@ -105,6 +105,9 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), 512 / (large_row_
     const int a = a0 + rg;
     // digit sizes: b = q or q + 1 bits, as 2^b and 2^-b
     const double pw0 = pow2(A.q), pw1 = pow2(A.q + 1), iv0 = pow2(-A.q), iv1 = pow2(-A.q - 1);
+    // column weight exponent sB(b) = (-2 R b p) mod N, from 32-bit products (N <= 2^23 < 2^32)
+    const uint32_t kB = (uint32_t)(2 * R) * (uint32_t)A.rem;
+    auto sB_of = [&](int b) { return (int)((0u - kB * (uint32_t)b) & (uint32_t)(N - 1)); };
 
     double2 v[E];
     double x0s[E], x1s[E];
@@ -159,7 +162,7 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), 512 / (large_row_
 #pragma unroll
             for (int i = 0; i < E; ++i) {
                 const int b = tr + TR * i;
-                const int sb = __ldg(A.sB + b);
+                const int sb = sB_of(b);
                 const double iwb = __ldg(A.iwB + b);
                 const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
                 const int s0 = o0 ? sA0 + sb - N : sA0 + sb, s1 = o1 ? sA1 + sb - N : sA1 + sb;
@@ -181,7 +184,7 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), 512 / (large_row_
 #pragma unroll
                 for (int i = 0; i < E; ++i) {
                     const int b = tr + TR * i;
-                    const int sb = __ldg(A.sB + b);
+                    const int sb = sB_of(b);
                     const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
                     const int s0 = o0 ? sA0 + sb - N : sA0 + sb, s1 = o1 ? sA1 + sb - N : sA1 + sb;
                     const bool w0 = s0 < A.rem, w1 = s1 < A.rem;
@@ -227,7 +230,7 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), 512 / (large_row_
                     const int b = tr + TR * i;
                     double cin = (blk > 0) ? __ldcg(A.carry + (size_t)(blk - 1) * C + b) : hin[b];
                     if (a == 0 && b == 0) cin -= 2.0;  // the "- 2" of s^2 - 2 (digit 0)
-                    const int sb = __ldg(A.sB + b);
+                    const int sb = sB_of(b);
                     const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
                     const int s0 = o0 ? sA0 + sb - N : sA0 + sb, s1 = o1 ? sA1 + sb - N : sA1 + sb;
                     const bool w0 = s0 < A.rem, w1 = s1 < A.rem;
@@ -278,7 +281,7 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), 512 / (large_row_
 #pragma unroll
     for (int i = 0; i < E; ++i) {
         const int b = tr + TR * i;
-        const int sb = __ldg(A.sB + b);
+        const int sb = sB_of(b);
         const double wb = __ldg(A.wB + b);
         const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
         v[i].x = x0s[i] * (wa0 * wb) * (o0 ? 0.5 : 1.0);

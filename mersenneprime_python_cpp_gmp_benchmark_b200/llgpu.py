@@ -365,6 +365,7 @@ def _main(argv=None):
     a.add_argument("--iters", type=int, default=8)
     a.add_argument("--n", type=int, default=0)
     a.add_argument("--engine", choices=tuple(ENGINES), default="fp64")
+    a.add_argument("--shape", default="", help="two-pass FP64 shape 'log2 row length,rows per block'")
     b = sub.add_parser("batch", help="whole Lucas-Lehmer tests of every prime in [lo, hi]")
     b.add_argument("--lo", type=int, required=True)
     b.add_argument("--hi", type=int, required=True)
@@ -373,6 +374,10 @@ def _main(argv=None):
     args = ap.parse_args(argv)
     t0 = time.perf_counter()
     if args.cmd == "square":
+        if args.shape:
+            c, g = (int(x) for x in args.shape.split(","))
+            n = args.n or fft_length(args.p)
+            set_large_split(n.bit_length() - 1, c, g)
         t = Test(args.p, args.n, args.engine)
         t.start()
         if args.iters > 1:
