@@ -97,7 +97,6 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), 512 / (large_row_
         }
         s_err = 0ull;
     }
-    for (int k = t; k < QL; k += T) qtw[k] = A.qtwC[k];
     __syncthreads();
     const int blk = s_blk;
     const unsigned ep = s_epoch;
@@ -121,6 +120,8 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), 512 / (large_row_
             x0s[i] = (double)d.x;
             x1s[i] = (double)d.y;
         }
+        for (int k = t; k < QL; k += T) qtw[k] = A.qtwC[k];
+        __syncthreads();
     } else {
         double lerr = 0.0;
         // Phase 0 (block 0 only): the last block's rows R-G .. R-1 through the same inverse FFT
@@ -138,6 +139,9 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), 512 / (large_row_
                     const int qq = t + T * r, pos = qq / G, ra = qq % G;
                     tmp[r] = A.V[(size_t)pos * R + base + ra];
                 }
+                // the twiddle table (L2-resident) is fetched while the rows' loads are in flight
+                if (ph == 0 || blk != 0)
+                    for (int k = t; k < QL; k += T) qtw[k] = A.qtwC[k];
 #pragma unroll
                 for (int r = 0; r < G * C / T; ++r) {
                     const int qq = t + T * r, pos = qq / G, ra = qq % G;
