@@ -162,11 +162,12 @@ class L2Flush:
 
 def range_flops(results):
     """Algorithmic FP64 flops of the tests: 5 N log2 N per squaring (forward + inverse real FFT)."""
+    import math
     tot = 0.0
     for r in results:
         n = r["n"]
         if n >= 32:
-            tot += r["iters"] * 5.0 * n * (n.bit_length() - 1)
+            tot += r["iters"] * 5.0 * n * math.log2(n)
     return tot
 
 
@@ -220,7 +221,8 @@ def bench_range(args, rank, world):
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: every prime exponent p <= 100001 from the sieve, s_0 = 4",
         "config": {"workload": "range p<=100001 (9592 LL tests, batched whole-test kernels, FP64 IBDWT, "
-                               "pow2 N 32..8192 at <=18 bits/digit)",
+                               "N = {1,3,5} x 2^k from 32 to 6144 at <=18 bits/digit)",
+                   "lengths": {str(n): c for n, c in sorted(__import__("collections").Counter(r["n"] for r in res).items())},
                    "tests": len(ps_all), "l2": "flushed (512 MiB write) between steps",
                    "parallelism": f"independent tests split over {world} GPU(s) by squaring cost (replicas)"},
         "e2e": {"value": round(e2e, 2), "unit": "tests/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
