@@ -301,8 +301,13 @@ def bench_big(args, rank, world):
     flops_iter = 5.0 * n * 23
     dom, dom_us = ("row", row_us) if row_us >= col_us else ("column", col_us)
     traffic = NCU_TRAFFIC[args.engine][dom]
-    hbm_peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"] \
-        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
+    peaks_file = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_file):
+        hbm_peak = json.load(open(peaks_file))["hbm_gbs"]
+        peak_source = "measured (MEASURED_PEAKS.json hbm_gbs, burst copy)"
+    else:
+        hbm_peak = 6650.0
+        peak_source = "fallback: 6.65 TB/s, an earlier copy measurement on this GPU pool"
     achieved = bytes_iter / (us_iter * world * 1e-6) / 1e9  # per GPU
     fp64_peak = llgpu.measure_peak("fp64") / 1e12
     line = {
@@ -321,11 +326,13 @@ def bench_big(args, rank, world):
                    "parallelism": f"one independent test per GPU ({world} replica(s))"},
         "e2e": {"value": round(1e6 * t_e2e / k_e2e, 3), "unit": "us/iteration", "iters": k_e2e,
                 "call": ("lucaslehmer.fft_res64_after" if args.engine == "fp64" else "lucaslehmer.gmp_res64_after")
-                        + "(136279841, 2000): tables, s_0 upload, squarings, digits D2H, exact residue rebuild",
-                "h2d_bytes_per_step": 4 * n, "d2h_bytes_per_step": 4 * n},
+                        + "(136279841, 2000): tables, s_0 upload, squarings, exact residue rebuilt on the "
+                          "device, res64 back",
+                # s_0 as N int32 digits up; res64, the rebuild's flags and the control block back
+                "h2d_bytes_per_step": 4 * n, "d2h_bytes_per_step": 128},
         "roofline": {"bound": "hbm", "achieved": round(bytes_pass / (dom_us * 1e-6) / 1e9, 1), "peak": hbm_peak,
                      "unit": "GB/s", "frac": round(bytes_pass / (dom_us * 1e-6) / 1e9 / hbm_peak, 4),
-                     "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs, burst copy)",
+                     "peak_source": peak_source,
                      "traffic": traffic,
                      "kernel": f"{dom} pass ({'large' if args.engine == 'fp64' else 'ntt'}_{'row' if dom == 'row' else 'col'})",
                      "kernel_us": round(dom_us, 2), "row_us": round(row_us, 2), "col_us": round(col_us, 2),

@@ -143,6 +143,14 @@ void llg_test_destroy(llg_test* t);
 int llg_residue_from_digits(uint64_t p, uint32_t n, const int64_t* digits, uint64_t* words,
                             size_t nwords, uint64_t* res64, int32_t* is_zero);
 
+/* The same residue from digits already on the device (int32, natural order, as the two-pass
+ * engine's final pass and llg_run_noalloc leave them), rebuilt on the GPU: word sums, a scan of the
+ * +-1 carry chains, the fold of the bits above p into bit 0, the canonical zero. d_words (device,
+ * ceil(p/64) words) may be null when only res64 / is_zero are wanted. Waits on `stream`.
+ * Replaces the same GMP rebuild without copying the digits back. */
+int llg_residue_from_digits_device(uint64_t p, uint32_t n, const int32_t* d_digits, uint64_t* d_words,
+                                   uint64_t* res64, int32_t* is_zero, void* stream);
+
 /* The two-pass engine for transform lengths 16,384 .. 65,536 without allocating device memory.
  * No counterpart in the reference: it serves callers that cannot call cudaMalloc (a host
  * framework that owns every device allocation through its own pool, or code that must not risk

@@ -493,6 +493,33 @@ void load_tuning_once(int dev) {
 }
 cudaError_t init_large(NttLargeTest& T, uint64_t p, int l) { return T.init(p, l); }
 
+// The exact residue of a two-pass test's digits (on the device after its FINAL pass), rebuilt on
+// the GPU; the words come back to the host only when asked for (into a vector or a caller buffer).
+int device_residue(uint64_t p, uint32_t n, const int* d_digits, std::vector<uint64_t>* vec, uint64_t* host,
+                   size_t host_cap, uint64_t* res64, int32_t* z, cudaStream_t st) {
+    const size_t nw = (size_t)((p + 63) / 64);
+    uint64_t* dw = nullptr;
+    if (vec || host) CK(cudaMallocAsync(&dw, nw * sizeof(uint64_t), st));
+    int rc = llg_residue_from_digits_device(p, n, d_digits, dw, res64, z, st);
+    if (rc) rc = fail(rc, "residue rebuild on the device failed");
+    if (!rc && dw) {
+        uint64_t* dst = host;
+        if (vec) {
+            vec->assign(nw, 0);
+            dst = vec->data();
+        }
+        if (cudaMemcpyAsync(dst, dw, nw * sizeof(uint64_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            rc = fail(LLG_E_CUDA, "copying the residue words back");
+        if (host)
+            for (size_t i = nw; i < host_cap; ++i) host[i] = 0;
+    }
+    if (dw) cudaFreeAsync(dw, st);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(st));
+    return LLG_OK;
+}
+
 template <class TestT>
 int run_large_t(const Item& item, llg_result& r, std::vector<uint64_t>* words, cudaStream_t st) {
     uint32_t n = item.n;
@@ -522,9 +549,8 @@ int run_large_t(const Item& item, llg_result& r, std::vector<uint64_t>* words, c
             worst = bits_to_double(h.err_max);
             if (worst > kAbortErrLarge) abort = true;
         }
-        std::vector<int> digits;
         if (!abort) {
-            CK(T.finish(st, digits));
+            CK(T.final_pass(st));
             CK(cudaEventRecord(e1, st));
             LargeCtl h;
             CK(T.read_ctl(h, st));
@@ -551,13 +577,13 @@ int run_large_t(const Item& item, llg_result& r, std::vector<uint64_t>* words, c
         }
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, e0, e1));
-        std::vector<int64_t> d64(digits.begin(), digits.end());
-        const size_t nw = (size_t)((item.p + 63) / 64);
-        std::vector<uint64_t> w(nw);
         int32_t z = 0;
-        const int rc = llg_residue_from_digits(item.p, n, d64.data(), w.data(), nw, &r.res64, &z);
-        if (rc) return rc;
-        if (words) *words = std::move(w);
+        const int rc = device_residue(item.p, n, T.digits, words, nullptr, 0, &r.res64, &z, st);
+        if (rc) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return rc;
+        }
         r.iters = item.iters;
         r.is_zero = z;
         r.n = n;
@@ -978,13 +1004,12 @@ int llg_test_read(llg_test* t, void* stream, llg_result* out, uint64_t* words, s
     const size_t nw = (size_t)((p + 63) / 64);
     if (words && nwords < nw) return fail(LLG_E_ARG, "words buffer too small");
     cudaStream_t st = stream ? (cudaStream_t)stream : default_stream_for_thread();
-    std::vector<int> digits;
     LargeCtl h;
     if (t->f) {
-        CK(t->f->finish(st, digits));
+        CK(t->f->final_pass(st));
         CK(t->f->read_ctl(h, st));
     } else {
-        CK(t->n->finish(st, digits));
+        CK(t->n->final_pass(st));
         CK(t->n->read_ctl(h, st));
     }
     std::memset(out, 0, sizeof *out);
@@ -993,9 +1018,9 @@ int llg_test_read(llg_test* t, void* stream, llg_result* out, uint64_t* words, s
     out->n = 1u << t->logN();
     out->max_err = bits_to_double(h.err_max);
     if (h.timeout) return fail(LLG_E_TIMEOUT, "carry wait timed out");
-    std::vector<int64_t> d64(digits.begin(), digits.end());
     int32_t z = 0;
-    int rc = llg_residue_from_digits(p, out->n, d64.data(), words, words ? nwords : 0, &out->res64, &z);
+    const int* dd = t->f ? t->f->digits : t->n->digits;
+    const int rc = device_residue(p, out->n, dd, nullptr, words, words ? nwords : 0, &out->res64, &z, st);
     if (rc) return rc;
     out->is_zero = z;
     out->status = out->max_err > kAbortErrLarge ? LLG_E_ROUNDOFF : LLG_OK;

@@ -49,6 +49,7 @@ struct LargeTest {
     cudaError_t start(const std::vector<int>& digits, cudaStream_t st);  // INIT + first squaring
     cudaError_t step(uint64_t k, cudaStream_t st);                        // k more squarings
     cudaError_t step_plain(uint64_t k, bool dump_last, cudaStream_t st);
+    cudaError_t final_pass(cudaStream_t st);                              // FINAL: digits on device
     cudaError_t finish(cudaStream_t st, std::vector<int>& out);           // FINAL: digits to host
     cudaError_t read_ctl(LargeCtl& h, cudaStream_t st);
     cudaError_t clear_err_since(cudaStream_t st);
@@ -72,6 +73,7 @@ struct NttLargeTest {
     cudaError_t init(uint64_t p, int log_n);
     cudaError_t start(const std::vector<int>& digits, cudaStream_t st);
     cudaError_t step(uint64_t k, cudaStream_t st);
+    cudaError_t final_pass(cudaStream_t st);
     cudaError_t finish(cudaStream_t st, std::vector<int>& out);
     cudaError_t read_ctl(LargeCtl& h, cudaStream_t st);
     cudaError_t time_passes(uint64_t k, cudaStream_t st, double& row_us, double& col_us);

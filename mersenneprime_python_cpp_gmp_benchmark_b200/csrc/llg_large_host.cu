@@ -254,12 +254,17 @@ cudaError_t LargeTest::step(uint64_t k, cudaStream_t st) {
     return step_plain(left, false, st);
 }
 
-cudaError_t LargeTest::finish(cudaStream_t st, std::vector<int>& out) {
+cudaError_t LargeTest::final_pass(cudaStream_t st) {
     cudaError_t e;
     if ((e = launch_large_row(logC, rows, LARGE_FINAL, args, st))) return e;
     // the squarings may resume from this state at the same epoch: clear the flags FINAL set
     if ((e = cudaMemsetAsync(&ctl->halo_read, 0, sizeof(unsigned), st))) return e;
-    if ((e = cudaMemsetAsync(flags, 0, (size_t)nblocks * sizeof(unsigned), st))) return e;
+    return cudaMemsetAsync(flags, 0, (size_t)nblocks * sizeof(unsigned), st);
+}
+
+cudaError_t LargeTest::finish(cudaStream_t st, std::vector<int>& out) {
+    cudaError_t e;
+    if ((e = final_pass(st))) return e;
     out.resize(2 * M);
     if ((e = cudaMemcpyAsync(out.data(), digits, 2 * M * sizeof(int), cudaMemcpyDeviceToHost, st))) return e;
     return cudaStreamSynchronize(st);
@@ -548,11 +553,16 @@ cudaError_t NttLargeTest::step(uint64_t k, cudaStream_t st) {
     return cudaSuccess;
 }
 
-cudaError_t NttLargeTest::finish(cudaStream_t st, std::vector<int>& out) {
+cudaError_t NttLargeTest::final_pass(cudaStream_t st) {
     cudaError_t e;
     if ((e = launch_ntt_row(logC, LARGE_FINAL, args, st))) return e;
     if ((e = cudaMemsetAsync(&ctl->halo_read, 0, sizeof(unsigned), st))) return e;
-    if ((e = cudaMemsetAsync(args.flags, 0, (size_t)nblocks * sizeof(unsigned), st))) return e;
+    return cudaMemsetAsync(args.flags, 0, (size_t)nblocks * sizeof(unsigned), st);
+}
+
+cudaError_t NttLargeTest::finish(cudaStream_t st, std::vector<int>& out) {
+    cudaError_t e;
+    if ((e = final_pass(st))) return e;
     out.resize(N);
     if ((e = cudaMemcpyAsync(out.data(), digits, N * sizeof(int), cudaMemcpyDeviceToHost, st))) return e;
     return cudaStreamSynchronize(st);

@@ -76,6 +76,8 @@ def lib() -> ctypes.CDLL:
         L.llg_test_errlog.argtypes = [ctypes.c_void_p, P(ctypes.c_float), sz, P(sz)]
         L.llg_set_large_split.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.llg_get_large_split.argtypes = [ctypes.c_int, P(ctypes.c_int)]
+        L.llg_residue_from_digits_device.argtypes = [u64, u32, ctypes.c_void_p, ctypes.c_void_p, P(u64),
+                                                     P(ctypes.c_int32), ctypes.c_void_p]
         L.llg_test_time_passes.argtypes = [ctypes.c_void_p, u64, ctypes.c_void_p, P(ctypes.c_double),
                                            P(ctypes.c_double)]
         L.llg_test_destroy.argtypes = [ctypes.c_void_p]
@@ -333,6 +335,22 @@ def run_noalloc(p, iters, n, digits_dev_ptr, stream=0):
     _check(lib().llg_run_noalloc(p, iters, n, ctypes.c_void_p(digits_dev_ptr), ctypes.byref(err),
                                  ctypes.c_void_p(stream or None)))
     return err.value
+
+
+def residue_from_digits_device(p, n, digits_dev_ptr, want_words=False, stream=0):
+    """llg_residue_from_digits_device: the residue of n int32 digits in device memory, rebuilt on
+    the GPU. Returns (is_zero, res64, words or None); words go through a temporary device buffer."""
+    r64, z = ctypes.c_uint64(), ctypes.c_int32()
+    if not want_words:
+        _check(lib().llg_residue_from_digits_device(p, n, ctypes.c_void_p(digits_dev_ptr), None, ctypes.byref(r64),
+                                                    ctypes.byref(z), ctypes.c_void_p(stream or None)))
+        return bool(z.value), r64.value, None
+    import torch
+    dw = torch.empty(nwords(p), dtype=torch.int64, device="cuda")
+    _check(lib().llg_residue_from_digits_device(p, n, ctypes.c_void_p(digits_dev_ptr), ctypes.c_void_p(dw.data_ptr()),
+                                                ctypes.byref(r64), ctypes.byref(z), ctypes.c_void_p(stream or None)))
+    words = [w & 0xFFFFFFFFFFFFFFFF for w in dw.cpu().tolist()]
+    return bool(z.value), r64.value, words
 
 
 def residue_from_digits(p, n, digits):

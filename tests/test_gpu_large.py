@@ -236,3 +236,28 @@ def test_splits_p136279841_res64(gpu):
             assert r["res64"] == after[(136279841, 1000)], c
     finally:
         gpu.set_large_split(23, -1)
+
+
+def test_device_residue_rebuild_matches_host(gpu):
+    """llg_residue_from_digits_device against the host rebuild on the same digits: random digits
+    of every size class (balanced, wide, tiny), the edge values (zero, 2^p - 1 == 0, -1), one-word
+    and large residues, power-of-two and 3 x 2^k lengths."""
+    import random
+    import torch
+    rng = random.Random(5)
+    cases = [(61, 4), (127, 32), (4423, 256), (44497, 3072), (330017, 16384), (1257787, 65536),
+             (22000007, 1 << 20)]
+    for p, n in cases:
+        b = -(-p // n)
+        for spread in (1 << (b - 1), 1 << min(b + 12, 30), 3):
+            d = [rng.randint(-spread, spread) for _ in range(n)]
+            dd = torch.tensor(d, dtype=torch.int32, device="cuda")
+            got = gpu.residue_from_digits_device(p, n, dd.data_ptr(), want_words=True)
+            want = gpu.residue_from_digits(p, n, d)
+            assert got == want, (p, n, spread)
+            assert gpu.residue_from_digits_device(p, n, dd.data_ptr())[:2] == want[:2]
+    p, n = 127, 32
+    bits = [-(-((j + 1) * p) // n) - (-(-(j * p) // n)) for j in range(n)]
+    for d in ([0] * n, [(1 << x) - 1 for x in bits], [-1] + [0] * (n - 1), [1 << 30] * n, [-(1 << 30)] * n):
+        dd = torch.tensor(d, dtype=torch.int32, device="cuda")
+        assert gpu.residue_from_digits_device(p, n, dd.data_ptr(), want_words=True) == gpu.residue_from_digits(p, n, d)
