@@ -1,4 +1,4 @@
-// Two-pass FP64 IBDWT squaring for N = 2^16 .. 2^23 with the residue resident in HBM.
+// Two-pass FP64 IBDWT squaring for N = 2^14 .. 2^23 with the residue resident in HBM.
 //
 // The M = N/2 packed complex values u_m (m = a + R*b: row a < R, column b < C, M = R*C) are
 // transformed by the four-step method. One squaring is two kernels, i.e. two read+write sweeps of
@@ -7,7 +7,7 @@
 // lucaslehmer.cpp:283,288, and an O(N) host loop for each of weight, unweight and carry,
 // lucaslehmer.cpp:282,289-310):
 //
-//   row pass (one block = kRowG consecutive rows, all C columns):
+//   row pass (one block = G consecutive rows, G = 2, 4 or 8, all C columns):
 //       inverse C-point FFT                                   (end of the previous squaring)
 //       unweight, round, max round-off, carry, "- 2"
 //       weight, forward C-point FFT                           (start of this squaring)
@@ -16,7 +16,7 @@
 //       (k, M-k), inverse R-point FFT, twiddle w_M^{-ac}
 //
 // The state is stored column-slot-major (element (a, pos) at pos*R + a), so a row block reads
-// and writes kRowG contiguous complex values (128 bytes) per column slot and a column block reads
+// and writes G contiguous complex values (16 G bytes) per column slot and a column block reads
 // and writes its columns contiguously.
 //
 // Carry. Digits 2m, 2m+1 of row a carry into row a+1 (m -> m+1 is a -> a+1), so the chain runs
@@ -27,7 +27,8 @@
 // memory; between blocks block k publishes its last row's carry-outs and a flag, and block k+1
 // reads them after a bounded wait. Blocks take tickets in launch order, so the block waited on is
 // always resident or finished. The wrap-around carry into row 0 (2^p == 1) comes from row R-1;
-// block 0 recomputes that row itself instead of waiting on the last block.
+// block 0 runs the last block's rows through the same code first, instead of waiting on the last
+// block, and the last block waits (bounded) until block 0 has read them before overwriting them.
 #include <cuda_runtime.h>
 
 #include <cstdint>
