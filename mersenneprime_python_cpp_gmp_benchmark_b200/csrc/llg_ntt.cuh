@@ -19,28 +19,79 @@ namespace gl {
 constexpr uint64_t Q = 0xFFFFFFFF00000001ull;
 constexpr uint64_t EPS = 0xFFFFFFFFull;  // 2^64 mod q
 
+// a + b for canonical a, b: the 65-bit sum with its carry c, and s + EPS with its carry; the
+// result is s + EPS when either carried (a carry means a + b - 2^64 + EPS = a + b - q; a carry of
+// s + EPS alone means s >= q), else s. 32-bit add-with-carry chains.
 __device__ __forceinline__ uint64_t add(uint64_t a, uint64_t b) {
-    uint64_t s = a + b;
-    s += (s < a) ? EPS : 0ull;  // 2^64 == EPS; cannot wrap again
-    return (s >= Q) ? s - Q : s;
+    uint64_t r;
+    asm("{\n\t.reg .u32 a0, a1, b0, b1, s0, s1, t0, t1, c, z;\n\t.reg .pred p;\n\t"
+        "mov.u32 z, 0;\n\t"
+        "mov.b64 {a0, a1}, %1;\n\t"
+        "mov.b64 {b0, b1}, %2;\n\t"
+        "add.cc.u32 s0, a0, b0;\n\t"
+        "addc.cc.u32 s1, a1, b1;\n\t"
+        "addc.u32 c, z, z;\n\t"
+        "add.cc.u32 t0, s0, 0xFFFFFFFF;\n\t"
+        "addc.cc.u32 t1, s1, z;\n\t"
+        "addc.u32 c, c, z;\n\t"
+        "setp.ne.u32 p, c, 0;\n\t"
+        "selp.b32 s0, t0, s0, p;\n\t"
+        "selp.b32 s1, t1, s1, p;\n\t"
+        "mov.b64 %0, {s0, s1};\n\t}"
+        : "=l"(r)
+        : "l"(a), "l"(b));
+    return r;
 }
 
+// a - b for canonical a, b: on a borrow, a - b + 2^64 - EPS = a - b + q
 __device__ __forceinline__ uint64_t sub(uint64_t a, uint64_t b) {
-    const uint64_t d = a - b;
-    return (a < b) ? d - EPS : d;  // a - b + 2^64 - EPS == a - b + q
+    uint64_t r;
+    asm("{\n\t.reg .u32 a0, a1, b0, b1, d0, d1, br, z;\n\t"
+        "mov.u32 z, 0;\n\t"
+        "mov.b64 {a0, a1}, %1;\n\t"
+        "mov.b64 {b0, b1}, %2;\n\t"
+        "sub.cc.u32 d0, a0, b0;\n\t"
+        "subc.cc.u32 d1, a1, b1;\n\t"
+        "subc.u32 br, z, z;\n\t"      // 0, or 0xFFFFFFFF = EPS after a borrow
+        "sub.cc.u32 d0, d0, br;\n\t"
+        "subc.u32 d1, d1, z;\n\t"
+        "mov.b64 %0, {d0, d1};\n\t}"
+        : "=l"(r)
+        : "l"(a), "l"(b));
+    return r;
 }
 
 __device__ __forceinline__ uint64_t neg(uint64_t a) { return a ? Q - a : 0ull; }
 
-// (hi * 2^64 + lo) mod q with hi = h1 * 2^32 + h0:  lo - h1 + h0 * (2^32 - 1)
+// (hi * 2^64 + lo) mod q with hi = h1 * 2^32 + h0:  lo - h1 + h0 * (2^32 - 1), canonical.
+// t = lo - h1 (minus EPS on a borrow: no second borrow since h1 < 2^32), u = h0 2^32 - h0,
+// r = t + u with the same carry / canonical step as add (r + EPS when t + u or r + EPS carries).
 __device__ __forceinline__ uint64_t reduce128(uint64_t lo, uint64_t hi) {
-    const uint64_t h1 = hi >> 32, h0 = hi & EPS;
-    uint64_t t = lo - h1;
-    if (lo < h1) t -= EPS;
-    const uint64_t u = (h0 << 32) - h0;
-    uint64_t r = t + u;
-    if (r < t) r += EPS;
-    return (r >= Q) ? r - Q : r;
+    uint64_t r;
+    asm("{\n\t.reg .u32 l0, l1, h0, h1, t0, t1, u0, u1, r0, r1, s0, s1, br, c, z;\n\t.reg .pred p;\n\t"
+        "mov.u32 z, 0;\n\t"
+        "mov.b64 {l0, l1}, %1;\n\t"
+        "mov.b64 {h0, h1}, %2;\n\t"
+        "sub.cc.u32 t0, l0, h1;\n\t"
+        "subc.cc.u32 t1, l1, z;\n\t"
+        "subc.u32 br, z, z;\n\t"
+        "sub.cc.u32 t0, t0, br;\n\t"
+        "subc.u32 t1, t1, z;\n\t"
+        "sub.cc.u32 u0, z, h0;\n\t"
+        "subc.u32 u1, h0, z;\n\t"
+        "add.cc.u32 r0, t0, u0;\n\t"
+        "addc.cc.u32 r1, t1, u1;\n\t"
+        "addc.u32 c, z, z;\n\t"
+        "add.cc.u32 s0, r0, 0xFFFFFFFF;\n\t"
+        "addc.cc.u32 s1, r1, z;\n\t"
+        "addc.u32 c, c, z;\n\t"
+        "setp.ne.u32 p, c, 0;\n\t"
+        "selp.b32 r0, s0, r0, p;\n\t"
+        "selp.b32 r1, s1, r1, p;\n\t"
+        "mov.b64 %0, {r0, r1};\n\t}"
+        : "=l"(r)
+        : "l"(lo), "l"(hi));
+    return r;
 }
 
 // a * b mod q, the 128-bit product from 32-bit multiply-adds
