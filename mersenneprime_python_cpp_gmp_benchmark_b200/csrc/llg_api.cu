@@ -134,7 +134,7 @@ int get_ntt(int dev, int log_n, const uint64_t** qtw, NttConst* K) {
         uint64_t omega;
         NttConst k;
         if (!ntt_constants(log_n, omega, k)) return fail(LLG_E_UNSUPPORTED, "no N-th root of 2 for N=2^%d", log_n);
-        const uint32_t QL = (1u << log_n) / 4;
+        const uint32_t QL = (1u << log_n) / 2;  // half table
         std::vector<uint64_t> h(gl_qpad8_len(QL), 0ull);
         uint64_t w = 1;
         for (uint32_t r = 0; r < QL; ++r) {

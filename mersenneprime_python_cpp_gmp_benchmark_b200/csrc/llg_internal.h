@@ -45,7 +45,7 @@ struct NttConst {
     uint64_t root2, inv_root2, invN;
 };
 
-// Exact NTT whole-test kernel, N = 2^log_n with 5 <= log_n <= 13 (qtw: padded quarter table of the
+// Exact NTT whole-test kernel, N = 2^log_n with 5 <= log_n <= 13 (qtw: padded half table of the
 // N-point transform, gl::qpad8 layout).
 cudaError_t launch_small_ntt(int log_n, const SmallJob* jobs, int njobs, const uint64_t* qtw, NttConst K,
                              int64_t* digits, SmallResult* results, cudaStream_t st);
@@ -130,8 +130,8 @@ cudaError_t launch_large_col(int log_r, const LargeArgs& a, cudaStream_t st);
 
 struct NttLargeArgs {
     uint64_t* V;              // state: element (row a, column slot pos) at pos * R + a
-    const uint64_t* qtwC;     // padded quarter table of the C-point row NTT (gl::qpad8)
-    const uint64_t* qtwR;     // padded quarter table of the R-point column NTT
+    const uint64_t* qtwC;     // padded half table of the C-point row NTT (gl::qpad8)
+    const uint64_t* qtwR;     // padded half table of the R-point column NTT
     const uint64_t* tw1;      // w_N^x, x < 2^tw_shift
     const uint64_t* tw2;      // w_N^(y 2^tw_shift)
     const int* pos_of_c;      // column slot of row-NTT frequency c

@@ -364,8 +364,8 @@ int ntt_pos_of_freq(int log_l, int k) {  // SmallGeom<log_l> (16 values per thre
     return rest * RLAST + klast;
 }
 
-std::vector<uint64_t> ntt_quarter(int log_l) {  // w_L^r at gl::qpad8(r), r < L/4
-    const uint32_t L = 1u << log_l, QL = L / 4;
+std::vector<uint64_t> ntt_half(int log_l) {  // w_L^r at gl::qpad8(r), r < L/2
+    const uint32_t L = 1u << log_l, QL = L / 2;
     std::vector<uint64_t> t(QL + (QL >> 4) + 1, 0ull);
     const uint64_t w = qpow(7, (kQ - 1) / L);
     uint64_t x = 1;
@@ -433,7 +433,7 @@ cudaError_t NttLargeTest::init(uint64_t p_, int log_n) {
     };
     NttLargeArgs& A = args;
     std::memset(&A, 0, sizeof A);
-    std::vector<uint64_t> qc = ntt_quarter(logC), qr = ntt_quarter(logR);
+    std::vector<uint64_t> qc = ntt_half(logC), qr = ntt_half(logR);
     std::vector<uint64_t> t1(1ull << s), t2(N >> s);
     {
         uint64_t x = 1;

@@ -215,25 +215,18 @@ struct NDft<16, INV> {
     __device__ __forceinline__ static void run(uint64_t* v) { NDftSplit<4, 4, INV>::run(v); }
 };
 
-// Quarter table of the L-point transform, stored padded (entry r at qpad8(r) = r + r/16: strided
-// pass indices spread over the 8-byte banks): t[qpad8(r)] = w_L^r, r < L/4. w_L^x for x < L is
-// w_4^quad * t[r] with w_4 = 2^48.
+// Half table of the L-point transform, stored padded (entry r at qpad8(r) = r + r/16: strided
+// pass indices spread over the 8-byte banks): t[qpad8(r)] = w_L^r, r < L/2. w_L^x for x < L is
+// t[x] or, past L/2, -t[x - L/2] (w_L^(L/2) = -1): a read and a negation, no further product.
 __host__ __device__ constexpr uint32_t qpad8(uint32_t r) { return r + (r >> 4); }
 __host__ __device__ constexpr uint32_t qpad8_len(uint32_t qm) { return qm + (qm >> 4) + 1; }
 
 template <int LOG_L>
 __device__ __forceinline__ uint64_t twiddle(const uint64_t* __restrict__ t, uint32_t x, bool inv) {
-    constexpr uint32_t L = 1u << LOG_L, QL = L / 4;
+    constexpr uint32_t L = 1u << LOG_L, HL = L / 2;
     if (inv) x = (L - x) & (L - 1);  // w^-x = w^(L - x)
-    const uint32_t quad = (x / QL) & 3u;
-    uint64_t w = t[qpad8(x % QL)];
-    switch (quad) {
-        case 0: break;
-        case 1: w = mul2k<48>(w); break;   // w_4 = 2^48
-        case 2: w = neg(w); break;         // w_4^2 = -1
-        default: w = mul2k<144>(w); break; // w_4^3 = 2^144
-    }
-    return w;
+    const uint64_t w = t[qpad8(x & (HL - 1))];
+    return (x & HL) ? neg(w) : w;
 }
 
 }  // namespace gl

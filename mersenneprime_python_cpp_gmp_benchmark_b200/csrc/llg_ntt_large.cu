@@ -42,10 +42,10 @@ __global__ void __launch_bounds__(kNttRowG * (1 << LOG_C) / 16, 2) ntt_row(const
     using GC = SmallG<LOG_C>;
     constexpr int C = GC::M, TR = GC::T, E = GC::E, G = kNttRowG, T = G * TR;
     constexpr int RS = GC::PAD + 1;  // odd row stride (8-byte slots): the G rows of a slot hit G banks
-    constexpr int QL = (int)gl::qpad8_len(C / 4);
+    constexpr int QL = (int)gl::qpad8_len(C / 2);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint64_t* bufs = reinterpret_cast<uint64_t*>(smem_raw);   // G exchange buffers
-    uint64_t* qtw = bufs + G * RS;                             // padded quarter table
+    uint64_t* qtw = bufs + G * RS;                             // padded half table
     int* carr2 = reinterpret_cast<int*>(qtw + QL + (QL & 1));  // G x C hop-2 carry-outs
     int* carr3 = carr2 + G * C;                                // G x C hop-3 carry-outs
     long long* carr1 = reinterpret_cast<long long*>(bufs);     // G x C hop-1 carry-outs (reuses bufs)
@@ -302,7 +302,7 @@ template <int LOG_R>
 __global__ void __launch_bounds__((1 << LOG_R) / 16, (LOG_R >= 13 ? 2 : 3)) ntt_col(const NttLargeArgs A) {
     using GR = SmallG<LOG_R>;
     constexpr int R = GR::M, TC = GR::T, E = GR::E;
-    constexpr int QL = (int)gl::qpad8_len(R / 4);
+    constexpr int QL = (int)gl::qpad8_len(R / 2);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint64_t* buf = reinterpret_cast<uint64_t*>(smem_raw);
     uint64_t* qtw = buf + GR::PAD;
@@ -343,14 +343,14 @@ __global__ void __launch_bounds__((1 << LOG_R) / 16, (LOG_R >= 13 ? 2 : 3)) ntt_
 template <int LOG_C>
 static size_t ntt_row_smem() {
     using GC = SmallGeom<LOG_C>;
-    const size_t ql = gl::qpad8_len(GC::M / 4);
+    const size_t ql = gl::qpad8_len(GC::M / 2);
     return sizeof(uint64_t) * (kNttRowG * (GC::PAD + 1) + ql + (ql & 1)) + 2 * sizeof(int) * kNttRowG * GC::M;
 }
 
 template <int LOG_R>
 static size_t ntt_col_smem() {
     using GR = SmallGeom<LOG_R>;
-    return sizeof(uint64_t) * (GR::PAD + gl::qpad8_len(GR::M / 4) + 2 * GR::E);
+    return sizeof(uint64_t) * (GR::PAD + gl::qpad8_len(GR::M / 2) + 2 * GR::E);
 }
 
 template <int LOG_C, int MODE>

@@ -28,10 +28,10 @@ __global__ void __launch_bounds__(SmallGeom<LOG_N>::T)
                  int64_t* __restrict__ digits_out, SmallResult* __restrict__ results) {
     using G = SmallG<LOG_N>;
     constexpr int N = G::M, E = G::E, T = G::T, W = G::W;
-    constexpr int QL = (int)gl::qpad8_len(N / 4);
+    constexpr int QL = (int)gl::qpad8_len(N / 2);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint64_t* buf = reinterpret_cast<uint64_t*>(smem_raw);  // exchange buffer, PAD slots
-    uint64_t* qtw = buf + G::PAD;                            // padded quarter table
+    uint64_t* qtw = buf + G::PAD;                            // padded half table
     uint64_t* wB = qtw + QL;                                 // E: w^sB(i)
     uint64_t* iwB = wB + E;                                  // E: w^-sB(i) / N
     long long* cbuf = reinterpret_cast<long long*>(iwB + E); // 3 hops x W x E carry slots
@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(SmallGeom<LOG_N>::T)
 template <int LOG_N>
 static size_t small_ntt_smem() {
     using G = SmallGeom<LOG_N>;
-    return sizeof(uint64_t) * (G::PAD + gl::qpad8_len(G::M / 4) + 2 * G::E) +
+    return sizeof(uint64_t) * (G::PAD + gl::qpad8_len(G::M / 2) + 2 * G::E) +
            sizeof(long long) * 3 * G::W * G::E + sizeof(int) * G::E;
 }
 
