@@ -42,10 +42,10 @@ STEP_ITERS = 1000  # squarings per timed step of the p=136,279,841 workload
 PASS_ITERS = 100   # squarings timed pass by pass for the dominant kernel's roofline
 # DRAM bytes (read + write) of one launch at p=136,279,841, N=2^23, from an ncu capture of
 # `python -m mersenneprime_python_cpp_gmp_benchmark_b200.llgpu square --p 136279841 --n 8388608
-# --iters 6 --shape 10,8` (the autotuned shape; profiles/two_pass_p136279841.md). The 64 MiB state
-# is partly L2-resident between the passes.
+# --iters 6 --shape 10,8` (the autotuned shape; NTT: `... --iters 6 --engine ntt`;
+# profiles/two_pass_p136279841.md). The 64 MiB state is partly L2-resident between the passes.
 NCU_TRAFFIC = {"fp64": {"row": 102667520, "column": 78124544},
-               "ntt": {"row": 118506752, "column": 105664000}}
+               "ntt": {"row": 115433728, "column": 94066176}}
 
 
 def sieve(lo, hi):
