@@ -59,6 +59,13 @@ __device__ __forceinline__ double2 twiddle_m(const double2* __restrict__ q, uint
     return inv ? conj2(r) : r;
 }
 
+// acc + a w + b conj(w): the radix-R0 terms of r and R0 - r share their factor up to conjugation
+// (w_R0^{(R0 - r) k} = conj(w_R0^{r k})), so the pair costs two sums and four multiply-adds.
+__device__ __forceinline__ double2 pair_term(double2 acc, double2 a, double2 b, double2 w) {
+    const double sx = a.x + b.x, sy = a.y + b.y, dx = a.x - b.x, dy = a.y - b.y;
+    return make_double2(fma(-dy, w.y, fma(sx, w.x, acc.x)), fma(dx, w.y, fma(sy, w.x, acc.y)));
+}
+
 }  // namespace
 
 template <int R0, int LOG_L>
@@ -151,7 +158,8 @@ __global__ void __launch_bounds__(MixedGeom<R0, LOG_L>::T, (MixedGeom<R0, LOG_L>
             const int n = tl + TL * i;
             double2 acc = bufs[phys(n)];
 #pragma unroll
-            for (int r = 1; r < R0; ++r) acc = cadd(acc, cmul(bufs[r * PADL + phys(n)], omf[seg * R0 + r]));
+            for (int r = 1; 2 * r < R0; ++r)
+                acc = pair_term(acc, bufs[r * PADL + phys(n)], bufs[(R0 - r) * PADL + phys(n)], omf[seg * R0 + r]);
             v[i] = cmul(acc, twiddle_m<M>(qtwM, (uint32_t)(n * seg), false));
         }
         __syncthreads();  // every segment read before the L-point FFTs overwrite the buffers
@@ -192,7 +200,8 @@ __global__ void __launch_bounds__(MixedGeom<R0, LOG_L>::T, (MixedGeom<R0, LOG_L>
             const int n = tl + TL * i;
             double2 acc = bufs[phys(n)];
 #pragma unroll
-            for (int k0 = 1; k0 < R0; ++k0) acc = cadd(acc, cmul(bufs[k0 * PADL + phys(n)], omi[seg * R0 + k0]));
+            for (int k0 = 1; 2 * k0 < R0; ++k0)
+                acc = pair_term(acc, bufs[k0 * PADL + phys(n)], bufs[(R0 - k0) * PADL + phys(n)], omi[seg * R0 + k0]);
             v[i] = acc;
         }
 
