@@ -69,7 +69,7 @@ __device__ __forceinline__ double2 pair_term(double2 acc, double2 a, double2 b, 
 }  // namespace
 
 template <int R0, int LOG_L>
-__global__ void __launch_bounds__(MixedGeom<R0, LOG_L>::T, (MixedGeom<R0, LOG_L>::T <= 96 ? 4 : MixedGeom<R0, LOG_L>::T <= 192 ? 2 : 1))
+__global__ void __launch_bounds__(MixedGeom<R0, LOG_L>::T, (MixedGeom<R0, LOG_L>::T <= 96 ? 4 : MixedGeom<R0, LOG_L>::T == 160 ? 3 : MixedGeom<R0, LOG_L>::T <= 192 ? 2 : 1))
     ll_small_fp64_mixed(const SmallJob* __restrict__ jobs, const double2* __restrict__ qtwL_g,
                         const double2* __restrict__ qtwM_g, int64_t* __restrict__ digits_out,
                         SmallResult* __restrict__ results, float* __restrict__ errlog, double abort_err) {
