@@ -77,6 +77,10 @@ struct NamedSync {
     __device__ __forceinline__ void operator()() const {
         asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
     }
+    // signal arrival without waiting (the producer side of a producer/consumer pair of warps)
+    __device__ __forceinline__ void arrive() const {
+        asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+    }
 };
 
 // Twiddle e^{-2 pi i x / M} (conjugated when inv) for geometry G, from its table.

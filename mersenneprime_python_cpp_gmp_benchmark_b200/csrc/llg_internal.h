@@ -65,6 +65,13 @@ constexpr bool large_rows_supported(int log_c, int g) {
            (g == 8 && log_c >= 9 && log_c <= 10);
 }
 constexpr int kLargeLogE = 4;         // log2 of the complex values per thread in the two-pass kernels
+// log2 of the complex values per thread in the row pass of g rows of 2^log_c complex: 8 values
+// (radix-8 passes, 64 registers a thread, two or more blocks per SM) for rows of up to 2^9, 16
+// (radix-16 passes, 128 registers) for longer rows
+#ifdef __CUDACC__
+__host__ __device__
+#endif
+constexpr int large_row_log_e(int log_c, int g) { return (void)g, log_c <= 9 ? 3 : 4; }
 
 struct LargeCtl {
     unsigned int epoch;              // squarings whose column pass has finished; +1 per column pass

@@ -25,7 +25,9 @@
 // the small remainder into the second, which keeps every digit within a few units of balanced and
 // makes carry-outs independent of carry-ins. Inside a block the carries pass through shared
 // memory; between blocks block k publishes its last row's carry-outs and a flag, and block k+1
-// reads them after a bounded wait. Blocks take tickets in launch order, so the block waited on is
+// reads them after a bounded wait. Only the block's first row waits for that flag (and its
+// second row for the first row's result): the other rows finish their carries from inside the
+// block and go on to the forward FFT meanwhile. Blocks take tickets in launch order, so the block waited on is
 // always resident or finished. The wrap-around carry into row 0 (2^p == 1) comes from row R-1;
 // block 0 runs the last block's rows through the same code first, instead of waiting on the last
 // block, and the last block waits (bounded) until block 0 has read them before overwriting them.
@@ -54,13 +56,22 @@ __device__ __forceinline__ double2 twiddle_M(const LargeArgs& A, uint32_t x, boo
 
 }  // namespace
 
-constexpr int large_row_threads(int log_c, int g) { return g * (1 << log_c) / (1 << kLargeLogE); }
+__host__ __device__ constexpr int large_row_threads(int log_c, int g) {
+    return g * (1 << log_c) / (1 << large_row_log_e(log_c, g));
+}
+// blocks per SM the row kernel is built for: 128 registers a thread at 16 values, 64 at 8
+__host__ __device__ constexpr int large_row_min_blocks(int log_c, int g) {
+    const int t = large_row_threads(log_c, g) < 32 ? 32 : large_row_threads(log_c, g);
+    const int b = (large_row_log_e(log_c, g) >= 4 ? 512 : 1024) / t;
+    return b > 16 ? 16 : b;
+}
 
 template <int LOG_C, int G, int MODE>
-__global__ void __launch_bounds__(large_row_threads(LOG_C, G), 512 / (large_row_threads(LOG_C, G) < 32 ? 32 : large_row_threads(LOG_C, G)))
+__global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blocks(LOG_C, G))
     large_row(const LargeArgs A) {
-    using GC = SmallG<LOG_C, kLargeLogE, TW_FULL>;  // full twiddle table
+    using GC = SmallG<LOG_C, large_row_log_e(LOG_C, G), TW_FULL>;  // full twiddle table
     constexpr int C = GC::M, TR = GC::T, E = GC::E, T = G * TR;
+    static_assert(T % 32 == 0, "whole warps");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int RS = GC::PAD + 1;  // row-buffer stride: odd, so the rows of a slot hit different banks
     constexpr int QL = (int)twiddle_table_len<GC>();
@@ -68,6 +79,7 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), 512 / (large_row_
     double2* qtw = bufs + G * RS;                            // padded twiddle table (C-point)
     double* carr = reinterpret_cast<double*>(bufs);          // G x C hop-1 carry-outs (reuses bufs)
     double* carr2 = carr + G * C;                            // G x C hop-2 carry-outs
+    double* late = reinterpret_cast<double*>(qtw + QL);     // C: row 0's hop-2 carry-outs, for row 1
     double* hin = reinterpret_cast<double*>(A.halo);         // C: wrap carry into row 0 (hop 2)
     double* hin2 = hin + C;                                  // C: wrap carry into row 0 (hop 3)
     __shared__ unsigned long long s_err;
@@ -182,7 +194,10 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), 512 / (large_row_
                 x1s[i] = dsplit(rb + c, w1 ? iv1 : iv0, w1 ? pw1 : pw0, c);
                 carr[rg * C + b] = c;
             }
-            atomicMax(&s_err, (unsigned long long)__double_as_longlong(lerr));
+            // the block's round-off max: one shared atomic per warp
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) lerr = fmax(lerr, __shfl_xor_sync(0xffffffffu, lerr, o));
+            if ((t & 31) == 0) atomicMax(&s_err, (unsigned long long)__double_as_longlong(lerr));
             __syncthreads();
             // ---- hop 2 for rows fed from inside the block ----
             if (rg > 0) {
@@ -219,16 +234,38 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), 512 / (large_row_
                     A.carry[(size_t)blk * C + b] = carr[(G - 1) * C + b];
                     A.carry2[(size_t)blk * C + b] = (float)carr2[(G - 1) * C + b];
                 }
+                __threadfence();  // each writer orders its carry-out stores before the flag below
             }
-            __threadfence();  // each writer orders its carry-out stores before the flag below
             __syncthreads();
+            // ---- hop 3 for rows 2 .. G-1: the small second-digit carry of the row above ----
+            if (rg >= 2) {
+#pragma unroll
+                for (int i = 0; i < E; ++i) x0s[i] += carr2[(rg - 1) * C + tr + TR * i];
+            }
             if (t == 0) {
                 __threadfence();
                 *reinterpret_cast<volatile unsigned*>(&A.flags[blk]) = ep + 1u;
-                if (blk > 0) wait_flag(&A.flags[blk - 1], ep + 1u, A.ctl, kSpinLimit);  // block blk-1's carries
+                const unsigned long long eb = s_err;
+                atomicMax(&A.ctl->err_max, eb);
+                atomicMax(&A.ctl->err_since, eb);
+                if (A.errlog) atomicMax(reinterpret_cast<unsigned int*>(A.errlog + (ep % (unsigned)A.errlog_len)),
+                                        __float_as_uint((float)__longlong_as_double((long long)eb)));
             }
+            // The carry arrays are read: each row may now reuse its exchange buffer, and rows
+            // 2 .. G-1 go on to the forward FFT. Row 0 waits for the previous block's carry-outs
+            // (hop 2 and 3 from outside the block); row 1 waits for row 0's hop-2 carry-outs,
+            // which pass through `late` (outside the exchange buffers).
             __syncthreads();
-            // ---- hop 2 for the block's first row: previous block's last row, or the wrap ----
+            if constexpr (TR >= 32) {
+                if (rg == 0) {
+                    if (t == 0 && blk > 0) wait_flag(&A.flags[blk - 1], ep + 1u, A.ctl, kSpinLimit);
+                    NamedSync{1u, (unsigned)TR}();
+                }
+            } else {
+                if (t == 0 && blk > 0) wait_flag(&A.flags[blk - 1], ep + 1u, A.ctl, kSpinLimit);
+                __syncthreads();
+            }
+            // ---- hop 2 and 3 for the block's first row: previous block's last row, or the wrap ----
             if (rg == 0) {
 #pragma unroll
                 for (int i = 0; i < E; ++i) {
@@ -242,22 +279,24 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), 512 / (large_row_
                     double c;
                     x0s[i] = dsplit(x0s[i] + cin, w0 ? iv1 : iv0, w0 ? pw1 : pw0, c);
                     x1s[i] = dsplit(x1s[i] + c, w1 ? iv1 : iv0, w1 ? pw1 : pw0, c);
-                    carr2[b] = c;
+                    late[b] = c;
+                    x0s[i] += (blk > 0) ? (double)__ldcg(A.carry2 + (size_t)(blk - 1) * C + b) : hin2[b];
                 }
             }
-            __syncthreads();
-            // ---- hop 3: the small second-digit carry of the previous row into this row's first digit
+            if constexpr (TR >= 32) {
+                if (rg == 0) {
+                    __threadfence_block();
+                    NamedSync{(unsigned)G + 1u, 2u * TR}.arrive();
+                } else if (rg == 1) {
+                    NamedSync{(unsigned)G + 1u, 2u * TR}();
+                }
+            } else {
+                __syncthreads();
+            }
+            // ---- hop 3 for row 1 ----
+            if (rg == 1) {
 #pragma unroll
-            for (int i = 0; i < E; ++i) {
-                const int b = tr + TR * i;
-                double c2;
-                if (rg > 0)
-                    c2 = carr2[(rg - 1) * C + b];
-                else if (blk > 0)
-                    c2 = (double)__ldcg(A.carry2 + (size_t)(blk - 1) * C + b);
-                else
-                    c2 = hin2[b];
-                x0s[i] += c2;
+                for (int i = 0; i < E; ++i) x0s[i] += late[tr + TR * i];
             }
             if (MODE == LARGE_FINAL || A.dump) {
 #pragma unroll
@@ -268,16 +307,8 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), 512 / (large_row_
                         make_int2(__double2int_rn(x0s[i]), __double2int_rn(x1s[i]));
                 }
             }
-            if (t == 0) {
-                const unsigned long long eb = s_err;
-                atomicMax(&A.ctl->err_max, eb);
-                atomicMax(&A.ctl->err_since, eb);
-                if (A.errlog) atomicMax(reinterpret_cast<unsigned int*>(A.errlog + (ep % (unsigned)A.errlog_len)),
-                                        __float_as_uint((float)__longlong_as_double((long long)eb)));
-            }
         }
         if constexpr (MODE == LARGE_FINAL) return;
-        __syncthreads();  // carry array reads done before the exchange buffers are reused
     }
 
     // ---- weight, forward row FFT, store ----
@@ -373,8 +404,8 @@ __global__ void __launch_bounds__(2 * (1 << LOG_R) / (1 << kLargeLogE), (LOG_R <
 
 template <int LOG_C, int G>
 static size_t row_smem() {
-    using GC = SmallG<LOG_C, kLargeLogE, TW_FULL>;
-    return sizeof(double2) * (G * (GC::PAD + 1) + twiddle_table_len<GC>());
+    using GC = SmallG<LOG_C, large_row_log_e(LOG_C, G), TW_FULL>;
+    return sizeof(double2) * (G * (GC::PAD + 1) + twiddle_table_len<GC>()) + sizeof(double) * GC::M;
 }
 
 template <int LOG_R>
@@ -405,7 +436,7 @@ static cudaError_t col_attr() {
 
 template <int LOG_C, int G, int MODE>
 static cudaError_t row_t(const LargeArgs& a, cudaStream_t st) {
-    large_row<LOG_C, G, MODE><<<a.nblocks, G * (1 << LOG_C) / (1 << kLargeLogE), row_smem<LOG_C, G>(), st>>>(a);
+    large_row<LOG_C, G, MODE><<<a.nblocks, large_row_threads(LOG_C, G), row_smem<LOG_C, G>(), st>>>(a);
     return cudaGetLastError();
 }
 

@@ -22,10 +22,10 @@ namespace llg {
 namespace {
 
 // column slot of row-FFT frequency k
-int host_pos_of_freq(int log_l, int k) {
-    // digit reversal of the row FFT's output positions (radix 2^kLargeLogE passes, the last one
-    // RLAST): host copy of pos_of_freq for SmallGeom<log_l, kLargeLogE>
-    const int LE = kLargeLogE, E = 1 << LE;
+int host_pos_of_freq(int log_l, int LE, int k) {
+    // digit reversal of the row FFT's output positions (radix 2^LE passes, the last one RLAST):
+    // host copy of pos_of_freq for SmallGeom<log_l, LE>
+    const int E = 1 << LE;
     const int L = 1 << log_l, P = (log_l + LE - 1) / LE;
     const int RLAST = (log_l % LE == 0) ? E : (1 << (log_l % LE));
     const int klast = k / (L / RLAST);
@@ -132,7 +132,7 @@ cudaError_t LargeTest::init(uint64_t p_, int log_n, int log_c, int rows_) {
     if ((e = upload(&tw1, omega_table(M, 1ull << s, 1)))) return e;
     if ((e = upload(&tw2, omega_table(M, M >> s, 1ull << s)))) return e;
     std::vector<int> pc(C);
-    for (int c = 0; c < C; ++c) pc[c] = host_pos_of_freq(logC, c);
+    for (int c = 0; c < C; ++c) pc[c] = host_pos_of_freq(logC, large_row_log_e(logC, rows), c);
     if ((e = upload(&pos_of_c, pc))) return e;
     std::vector<double> hwA(2 * R), hiwA(2 * R), hwB(C), hiwB(C);
     std::vector<int> hsA(2 * R), hsB(C);

@@ -86,9 +86,9 @@ Layout layout(int logN, int logC, int logR, int s) {
 }
 
 int pos_of_freq_host(int log_l, int k) {
-    // digit reversal of the row FFT's output positions (radix 2^kLargeLogE passes, the last one
-    // RLAST): host copy of pos_of_freq for SmallGeom<log_l, kLargeLogE>
-    const int LE = kLargeLogE, E = 1 << LE;
+    // digit reversal of the row FFT's output positions (radix 2^LE passes, the last one RLAST):
+    // host copy of pos_of_freq for SmallGeom<log_l, LE>, LE as the row kernel is built
+    const int LE = large_row_log_e(log_l, large_rows_per_block(log_l)), E = 1 << LE;
     const int L = 1 << log_l, P = (log_l + LE - 1) / LE;
     const int RLAST = (log_l % LE == 0) ? E : (1 << (log_l % LE));
     const int klast = k / (L / RLAST);
