@@ -58,10 +58,10 @@ constexpr int kRowG = 4;              // rows per row-pass block (rows of up to 
 __host__ __device__
 #endif
 constexpr int large_rows_per_block(int log_c) { return log_c >= 11 ? 2 : kRowG; }
-// row-pass shapes with kernels: 4 rows per block for rows of 2^6 .. 2^10, 2 rows for 2^8 .. 2^11,
+// row-pass shapes with kernels: 4 rows per block for rows of 2^6 .. 2^11, 2 rows for 2^8 .. 2^11,
 // 8 rows for 2^9 .. 2^10 (the larger the block, the longer the contiguous runs of its loads)
 constexpr bool large_rows_supported(int log_c, int g) {
-    return (g == 4 && log_c >= 6 && log_c <= 10) || (g == 2 && log_c >= 8 && log_c <= 11) ||
+    return (g == 4 && log_c >= 6 && log_c <= 11) || (g == 2 && log_c >= 8 && log_c <= 11) ||
            (g == 8 && log_c >= 9 && log_c <= 10);
 }
 constexpr int kLargeLogE = 4;         // log2 of the complex values per thread in the two-pass kernels

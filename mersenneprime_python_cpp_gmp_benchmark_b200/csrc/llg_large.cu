@@ -458,6 +458,7 @@ cudaError_t configure_large(int log_c, int g, int log_r) {
         case 16 * 8 + 4: e = row_attrs<8, 4>(); break;
         case 16 * 9 + 4: e = row_attrs<9, 4>(); break;
         case 16 * 10 + 4: e = row_attrs<10, 4>(); break;
+        case 16 * 11 + 4: e = row_attrs<11, 4>(); break;
         case 16 * 8 + 2: e = row_attrs<8, 2>(); break;
         case 16 * 9 + 2: e = row_attrs<9, 2>(); break;
         case 16 * 10 + 2: e = row_attrs<10, 2>(); break;
@@ -486,6 +487,7 @@ static cudaError_t row_mode(int log_c, int g, const LargeArgs& a, cudaStream_t s
         case 16 * 8 + 4: return row_t<8, 4, MODE>(a, st);
         case 16 * 9 + 4: return row_t<9, 4, MODE>(a, st);
         case 16 * 10 + 4: return row_t<10, 4, MODE>(a, st);
+        case 16 * 11 + 4: return row_t<11, 4, MODE>(a, st);
         case 16 * 8 + 2: return row_t<8, 2, MODE>(a, st);
         case 16 * 9 + 2: return row_t<9, 2, MODE>(a, st);
         case 16 * 10 + 2: return row_t<10, 2, MODE>(a, st);
