@@ -44,7 +44,7 @@ PASS_ITERS = 100   # squarings timed pass by pass for the dominant kernel's roof
 # `python -m mersenneprime_python_cpp_gmp_benchmark_b200.llgpu square --p 136279841 --n 8388608
 # --iters 6 --shape 10,8` (the autotuned shape; NTT: `... --iters 6 --engine ntt`;
 # profiles/two_pass_p136279841.md). The 64 MiB state is partly L2-resident between the passes.
-NCU_TRAFFIC = {"fp64": {"row": 102667520, "column": 78124544},
+NCU_TRAFFIC = {"fp64": {"row": 106451200, "column": 78296064},
                "ntt": {"row": 115433728, "column": 94066176}}
 
 
