@@ -7,11 +7,13 @@ Workloads (synthetic inputs: the exponents themselves, s_0 = 4; no dataset exist
   big     (default) p = 136,279,841 on the two-pass FP64 IBDWT engine at N = 2^23; one step = 1000
           squarings. metric: us per Lucas-Lehmer iteration (lower is better). value: CUDA events on
           the launch stream, the 64 MiB state resident on the device, L2 flushed between steps.
-          e2e: lucaslehmer.fft_res64_after(p, 2000) -- tables, upload of s_0, squarings, digits
-          back, exact residue on the host -- per squaring.
+          e2e: lucaslehmer.fft_res64_after(p, 2000) -- tables, upload of s_0, squarings, exact
+          residue rebuilt on the device, res64 back -- per squaring.
   range   every prime p <= 100,001 (9,592 Lucas-Lehmer tests, 28 Mersenne hits), batched whole-test
           kernels bucketed by transform length. One step = every test run to completion.
           metric: tests/s. e2e: lucaslehmer_cuda.lucas_lehmer_batch() on the host list.
+          batched_vs_plain: every prime p <= 10,001 one exponent per launch against one batched
+          launch, on the same GPU (device time, residues compared).
 --impl reference: the reference's own CPU engine (its lucaslehmer.cpp compiled unchanged into
 oracle/_ref/) on the host cores for the same metric: bench_square at p = 136,279,841 (big) or a
 stratified sample of the range (range).
@@ -171,6 +173,29 @@ def range_flops(results):
     return tot
 
 
+def plain_vs_batched(llgpu, hi=10001):
+    """Every prime p <= hi (1229 tests for 10001) as one exponent per launch, then as one batched
+    launch, on the same GPU: device time of the launches, residues compared."""
+    ps = sieve(2, hi)
+    batch = llgpu.Batch(ps)
+    batch.launch()
+    batch.device_ms()
+    batch.launch()
+    t_batch = batch.device_ms() * 1e-3
+    res = {r["p"]: r["res64"] for r in batch.results()}
+    batch.close()
+    t_plain = 0.0
+    for p in ps:
+        one = llgpu.Batch([p])
+        one.launch()
+        t_plain += one.device_ms() * 1e-3
+        assert one.results()[0]["res64"] == res[p], f"p={p}: per-exponent and batched residues differ"
+        one.close()
+    return {"tests": f"every prime p <= {hi} ({len(ps)} tests), one exponent per launch vs one batched launch",
+            "plain_tests_per_s": round(len(ps) / t_plain, 2), "batched_tests_per_s": round(len(ps) / t_batch, 2),
+            "batched_speedup": round(t_plain / t_batch, 2), "timing": "device time of the launches (CUDA events)"}
+
+
 def bench_range(args, rank, world):
     import torch
     from mersenneprime_python_cpp_gmp_benchmark_b200 import llgpu
@@ -234,6 +259,8 @@ def bench_range(args, rank, world):
         "hits": len(hits),
         "gpu_launches": args.steps * len({r["n"] for r in res}),
     }
+    if rank == 0:
+        line["batched_vs_plain"] = plain_vs_batched(llgpu)
     return line
 
 
