@@ -9,13 +9,13 @@
 //   X[R0 k' + k0] = sum_n w_L^{n k'} w_M^{n k0} sum_r u[n + L r] w_R0^{r k0}
 // so a squaring is: the radix-R0 step across the R0 segments (one shared-memory exchange) with the
 // twiddle w_M^{n k0}; R0 independent L-point FFTs (the power-of-two radix passes, one segment of
-// L/16 threads each, named barriers per segment); the real-FFT split and square on the pair
+// L/E threads each, named barriers per segment); the real-FFT split and square on the pair
 // (k, M - k), which pairs segment k0 with segment R0 - k0; the inverse L-point FFTs; the conjugate
 // twiddle and the inverse radix-R0 step; then unweight, round, carry and weight in registers.
 //
-// Thread t = seg * TL + tl holds u[seg L + tl + TL i], i < 16, between squarings: digit order runs
-// across the lanes of a segment, then to the next column i, then to the next segment, and wraps
-// from the last digit to digit 0 (2^p == 1). The carry-out of a thread does not depend on its
+// Thread t = seg * TL + tl holds u[seg L + tl + TL i], i < E (8 or 16), between squarings: digit
+// order runs across the lanes of a segment, then to the next column i, then to the next segment,
+// and wraps from the last digit to digit 0 (2^p == 1). The carry-out of a thread does not depend on its
 // carry-in (as in the power-of-two kernel), so one exchange per squaring suffices.
 #include <cuda_runtime.h>
 
@@ -29,9 +29,11 @@ namespace llg {
 
 namespace {
 
-template <int R0_, int LOG_L>
+// values per thread: 8 (radix-8 passes, twice the warps) where the L-point FFT needs no more
+// passes than with 16 (L = 2^9: 8 x 8 x 8 against 16 x 16 x 2), else 16
+template <int R0_, int LOG_L, int LE_ = (LOG_L == 9 ? 3 : 4)>
 struct MixedGeom {
-    using GL = SmallG<LOG_L, 4, TW_QUARTER>;
+    using GL = SmallG<LOG_L, LE_, TW_QUARTER>;
     static constexpr int R0 = R0_;
     static constexpr int L = GL::M, TL = GL::T, E = GL::E;
     static constexpr int M = R0 * L, N = 2 * M, T = R0 * TL;
@@ -66,10 +68,15 @@ __device__ __forceinline__ double2 pair_term(double2 acc, double2 a, double2 b, 
     return make_double2(fma(-dy, w.y, fma(sx, w.x, acc.x)), fma(dx, w.y, fma(sy, w.x, acc.y)));
 }
 
+// blocks per SM the kernel is built for (registers: 65536 / (blocks x threads) a thread)
+__host__ __device__ constexpr int mixed_min_blocks(int t, int e) {
+    return e == 16 ? (t <= 96 ? 4 : t == 160 ? 3 : t <= 192 ? 2 : 1) : (t <= 192 ? 4 : t <= 320 ? 2 : 1);
+}
+
 }  // namespace
 
 template <int R0, int LOG_L>
-__global__ void __launch_bounds__(MixedGeom<R0, LOG_L>::T, (MixedGeom<R0, LOG_L>::T <= 96 ? 4 : MixedGeom<R0, LOG_L>::T == 160 ? 3 : MixedGeom<R0, LOG_L>::T <= 192 ? 2 : 1))
+__global__ void __launch_bounds__(MixedGeom<R0, LOG_L>::T, mixed_min_blocks(MixedGeom<R0, LOG_L>::T, MixedGeom<R0, LOG_L>::E))
     ll_small_fp64_mixed(const SmallJob* __restrict__ jobs, const double2* __restrict__ qtwL_g,
                         const double2* __restrict__ qtwM_g, int64_t* __restrict__ digits_out,
                         SmallResult* __restrict__ results, float* __restrict__ errlog, double abort_err) {
@@ -191,7 +198,7 @@ __global__ void __launch_bounds__(MixedGeom<R0, LOG_L>::T, (MixedGeom<R0, LOG_L>
         //      u[n + L r] = sum_k0 w_R0^{-r k0} w_M^{-n k0} z[k0][n] ----
 #pragma unroll
         for (int i = 0; i < E; ++i) v[i] = cmul(v[i], twiddle_m<M>(qtwM, (uint32_t)((tl + TL * i) * seg), true));
-        __syncthreads();  // the last inverse pass read its segment buffer
+        gsync();  // this segment's last inverse pass read its buffer (no other segment reads it)
 #pragma unroll
         for (int i = 0; i < E; ++i) mybuf[phys(tl + TL * i)] = v[i];
         __syncthreads();
