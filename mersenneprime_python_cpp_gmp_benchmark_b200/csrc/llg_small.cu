@@ -7,8 +7,8 @@
 // single-block GPU loop of cuda/ll_ntt.cu:91-163, with a different transform:
 //
 //   * the N real weighted digits are packed as M = N/2 complex values u_m = y_2m + i y_2m+1 and
-//     transformed by an M-point complex FFT (radix-16 passes, in-register DFTs, one shared-memory
-//     exchange per pass, no bit reversal);
+//     transformed by an M-point complex FFT (radix-16 passes, radix-8 for M = 512, in-register
+//     DFTs, one shared-memory exchange per pass, no bit reversal);
 //   * the real-FFT split and the pointwise square are one step on the pair (k, M-k):
 //       U'_k = [(3A - B)(A + B) - w^k (A - B)^2] / 4,  A = U_k, B = conj(U_{M-k}), w = e^{-2 pi i/M}
 //     which equals DFT_M(z_even + i z_odd) for the cyclic square z = y * y;
@@ -33,12 +33,22 @@
 
 namespace llg {
 
+// log2 of the complex values per thread for M = 2^log_m: 8 (radix-8 passes, twice the warps)
+// for M = 2^9, where that takes no more passes than 16 (8 x 8 x 8 against 16 x 16 x 2); 16 else
+__host__ __device__ constexpr int small_log_e(int log_m) { return log_m == 9 ? 3 : 4; }
 template <int LOG_M>
-__global__ void __launch_bounds__(SmallGeom<LOG_M>::T, (SmallGeom<LOG_M>::T < 32 ? 16 : 512 / SmallGeom<LOG_M>::T))
+using SmallGeo = SmallG<LOG_M, small_log_e(LOG_M), TW_QUARTER>;
+// blocks per SM the kernel is built for: 128 registers a thread at 16 values, ~85 at 8
+__host__ __device__ constexpr int small_min_blocks(int t, int le) {
+    return t < 32 ? 16 : (le >= 4 ? 512 : 768) / t > 16 ? 16 : (le >= 4 ? 512 : 768) / t;
+}
+
+template <int LOG_M>
+__global__ void __launch_bounds__(SmallGeo<LOG_M>::T, small_min_blocks(SmallGeo<LOG_M>::T, small_log_e(LOG_M)))
     ll_small_fp64(const SmallJob* __restrict__ jobs, const double2* __restrict__ qtw_g,
                   int64_t* __restrict__ digits_out, SmallResult* __restrict__ results,
                   float* __restrict__ errlog, double abort_err) {
-    using G = SmallG<LOG_M, 4, TW_QUARTER>;
+    using G = SmallGeo<LOG_M>;
     constexpr int M = G::M, N = G::N, E = G::E, T = G::T, W = G::W;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2* buf = reinterpret_cast<double2*>(smem_raw);          // exchange buffer, PAD slots
@@ -323,7 +333,7 @@ cudaError_t launch_word(const SmallJob* jobs, int njobs, uint64_t* res, cudaStre
 
 template <int LOG_M>
 static size_t small_smem_bytes() {
-    using G = SmallG<LOG_M, 4, TW_QUARTER>;
+    using G = SmallGeo<LOG_M>;
     size_t b = sizeof(double2) * G::PAD;
     b += sizeof(double2) * twiddle_table_len<G>();
     b += 2 * sizeof(double) * G::E + sizeof(int) * (G::E + (G::E & 1 ? 1 : 0) + 2);
@@ -335,7 +345,7 @@ template <int LOG_M>
 static cudaError_t launch_small_t(const SmallJob* jobs, int njobs, const double2* qtw,
                                   int64_t* digits, SmallResult* results, float* errlog,
                                   double abort_err, cudaStream_t st) {
-    using G = SmallGeom<LOG_M>;
+    using G = SmallGeo<LOG_M>;
     const size_t smem = small_smem_bytes<LOG_M>();
     static bool configured = false;  // benign race: the attribute call is idempotent
     if (!configured) {
