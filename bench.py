@@ -14,6 +14,11 @@ Workloads (synthetic inputs: the exponents themselves, s_0 = 4; no dataset exist
           metric: tests/s. e2e: lucaslehmer_cuda.lucas_lehmer_batch() on the host list.
           batched_vs_plain: every prime p <= 10,001 one exponent per launch against one batched
           launch, on the same GPU (device time, residues compared).
+  single  p = 1,257,787 (a Mersenne exponent) at N = 65536, the whole test on the FP64 and NTT
+          engines: us per squaring, res64 every 10^4 squarings against the reference GMP trace,
+          final residue zero, the round-off maximum and per-squaring log.
+  sweep   8 seeded primes in [20M, 25M]: FP64 asked at N = 2^20 (escalating on round-off > 0.4)
+          against the NTT at its exact length; length used, escalations, round-off, us per squaring.
 --impl reference: the reference's own CPU engine (its lucaslehmer.cpp compiled unchanged into
 oracle/_ref/) on the host cores for the same metric: bench_square at p = 136,279,841 (big) or a
 stratified sample of the range (range).
@@ -378,6 +383,180 @@ def bench_big(args, rank, world):
     return line
 
 
+SINGLE_P, SINGLE_N = 1257787, 65536
+SWEEP_N = 1 << 20
+METRIC_SINGLE = "us/LL-iteration at p=1,257,787 (N=65536, whole test)"
+METRIC_SWEEP = "us/LL-iteration over 8 seeded primes in [20M,25M] (FP64 asked at N=2^20)"
+
+
+def bench_single(args, rank, world):
+    """p = 1,257,787 (a Mersenne exponent) at N = 65536 (19.19 bits/digit), every one of its p - 2
+    squarings, on the FP64 and the NTT two-pass engines. One step = the whole test. Per engine: us per
+    squaring from CUDA events around the squarings (the res64 reads every 10^4 squarings, checked
+    against the reference GMP trace, fall outside the events), the final residue (zero), and for
+    FP64 the run's worst round-off plus the per-squaring round-off log of its last 65536 squarings.
+    The 512 KiB state is L2-resident by design at this size."""
+    import torch
+    from mersenneprime_python_cpp_gmp_benchmark_b200 import llgpu
+    tr = json.load(open(os.path.join(ROOT, "tests", "golden", "trace_1257787.json")))
+    p, every = tr["p"], tr["every"]
+    assert p == SINGLE_P
+    stream = torch.cuda.Stream()
+    h = stream.cuda_stream
+    legs = {}
+    barrier(world)
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        for engine in ("fp64", "ntt"):
+            w = llgpu.Test(p, SINGLE_N, engine)  # warm-up: tables, graphs, clocks
+            w.start(h)
+            w.iterate(args.warmup * 1000, h)
+            torch.cuda.synchronize()
+            w.close()
+            t = llgpu.Test(p, SINGLE_N, engine)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+            def timed(fn):
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                e1.synchronize()
+                return e0.elapsed_time(e1) * 1e-3
+
+            elapsed = timed(lambda: t.start(h))
+            done, checked, mismatches = 1, 0, 0
+            for i, want in enumerate(tr["res64"]):
+                k = every * (i + 1)
+                elapsed += timed(lambda: t.iterate(k - done, h))
+                done = k
+                r = t.read(h)
+                checked += 1
+                mismatches += int(r["res64"] != int(want, 16))
+            elapsed += timed(lambda: t.iterate(p - 2 - done, h))
+            r = t.read(h)
+            assert r["iters"] == p - 2 and r["status"] == 0, r
+            assert mismatches == 0 and r["is_zero"] == 1, (engine, mismatches, r["res64"])
+            leg = {"us_per_iteration": round(1e6 * elapsed / (p - 2), 3), "seconds": round(elapsed, 3),
+                   "iterations": p - 2, "final_residue_zero": True,
+                   "res64_checked_every": every, "res64_checks": checked, "res64_mismatches": mismatches}
+            if engine == "fp64":
+                log = sorted(x for x in t.errlog(65536) if x > 0)
+                leg["max_roundoff"] = r["max_err"]
+                leg["roundoff_log_last_65536"] = {
+                    "max": log[-1], "p99": log[int(0.99 * (len(log) - 1))], "median": log[len(log) // 2]}
+            t.close()
+            legs[engine] = leg
+    lead = legs[args.engine]
+    t_max = max_over_ranks(lead["seconds"], world)
+    us_iter = 1e6 * t_max / ((p - 2) * world)
+    # e2e: the C-ABI call llg_run at the same length for an interim residue, host in / host out
+    k_e2e = 100000
+    llgpu.run(p, iters=1000, n=SINGLE_N, engine=args.engine)
+    t0 = time.perf_counter()
+    e2e_r = llgpu.run(p, iters=k_e2e, n=SINGLE_N, engine=args.engine)
+    t_e2e = max_over_ranks(time.perf_counter() - t0, world)
+    assert e2e_r["iters"] == k_e2e and e2e_r["n"] == SINGLE_N, e2e_r
+    return {
+        "metric": METRIC_SINGLE, "value": round(us_iter, 3), "unit": "us/iteration", "n_gpus": world,
+        "steps": 1, "warmup": args.warmup, "ms_per_step": round(1e3 * t_max, 3),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.engine == "fp64" else "u64 (GF(2^64-2^32+1))",
+        "data": "synthetic: the LL sequence of p=1,257,787 from s_0=4 (no external data)",
+        "config": {"workload": "p=1,257,787 whole test (1,257,785 squarings) at N=65536 (19.19 bits/digit), "
+                               "two-pass engine, FP64 and Goldilocks NTT; one step = the whole test",
+                   "engine": args.engine, "l2": "the 512 KiB state is L2-resident by design",
+                   "parallelism": f"one independent test per GPU ({world} replica(s))"},
+        "engines": legs,
+        "e2e": {"value": round(1e6 * t_e2e / k_e2e, 3), "unit": "us/iteration", "iters": k_e2e,
+                "call": f"llg_run(1257787, {k_e2e}, {args.engine}, n=65536) through the C-ABI: tables, s_0 upload, "
+                        "squarings, residue rebuilt on the device, result struct back",
+                "h2d_bytes_per_step": 4 * SINGLE_N, "d2h_bytes_per_step": 128},
+        "clocks": clk.summary(),
+        "gpu_launches": 2 * (p - 2),  # the reported engine's row and column pass per squaring
+    }
+
+
+def bench_sweep(args, rank, world):
+    """The 8 seeded primes of [20,000,000, 25,000,000] (sorted(random.Random(0).sample(primes, 8)),
+    as listed in tests/golden/appendix.json). FP64 is asked for N = 2^20 (19.4-23.4 bits/digit) and
+    escalates to the next length whenever the round-off passes 0.4; the NTT runs at its exact
+    length (2^20 up to p = 22,020,096, else 2^21). Per prime and engine: res64 after 1000
+    squarings against the reference GMP engine, then a run of K squarings through llg_run: the
+    length used, the escalations, the worst round-off and us per squaring (CUDA events of the
+    attempt that finished). value = FP64 us per squaring averaged over the 8 primes."""
+    from mersenneprime_python_cpp_gmp_benchmark_b200 import llgpu
+    g = json.load(open(os.path.join(ROOT, "tests", "golden", "appendix.json")))
+    gold = {(d["p"], d["k"]): int(d["res64"], 16) for d in g["after"]}
+    primes = g["sweep_primes"]
+    iters = {"fp64": args.sweep_iters, "ntt": args.sweep_ntt_iters}
+    rows, walls = [], {"fp64": 0.0, "ntt": 0.0}
+    llgpu.run(primes[0], iters=64 * args.warmup, n=SWEEP_N)  # warm-up
+    barrier(world)
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        for p in primes:
+            row = {"p": p, "bits_per_digit_at_2^20": round(p / SWEEP_N, 2)}
+            for engine in ("fp64", "ntt"):
+                n = SWEEP_N if engine == "fp64" else max(SWEEP_N, llgpu.ntt_length(p))
+                chk = llgpu.run(p, iters=1000, n=n, engine=engine)
+                match = chk["status"] == 0 and chk["res64"] == gold[(p, 1000)]
+                t0 = time.perf_counter()
+                r = llgpu.run(p, iters=iters[engine], n=n, engine=engine)
+                walls[engine] += time.perf_counter() - t0
+                assert r["status"] == 0, (p, engine, r)
+                row[engine] = {"n_used": r["n"], "escalations": r["escalations"],
+                               "max_roundoff": round(r["max_err"], 5),
+                               "us_per_iteration": round(1e6 * r["seconds"] / r["iters"], 3),
+                               "res64_after_1000_matches_reference": match}
+            rows.append(row)
+    us = {e: sum(r[e]["us_per_iteration"] for r in rows) / len(rows) for e in ("fp64", "ntt")}
+    esc = {e: sum(r[e]["escalations"] for r in rows) for e in ("fp64", "ntt")}
+    lead = args.engine
+    return {
+        "metric": METRIC_SWEEP, "value": round(us[lead], 3), "unit": "us/iteration", "n_gpus": world,
+        "steps": 1, "warmup": args.warmup, "ms_per_step": round(1e3 * walls[lead], 3),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if lead == "fp64" else "u64 (GF(2^64-2^32+1))",
+        "data": "synthetic: the LL sequences of 8 seeded primes from s_0=4 (no external data)",
+        "config": {"workload": f"precision sweep: 8 primes in [20M,25M], FP64 asked at N=2^20 (escalating on "
+                               f"round-off > 0.4) vs NTT at its exact length; {iters['fp64']} FP64 and "
+                               f"{iters['ntt']} NTT squarings timed per prime",
+                   "engine": lead, "l2": "state 16-32 MiB per test; one test at a time",
+                   "parallelism": "one GPU"},
+        "primes": rows,
+        "mean_us_per_iteration": {e: round(v, 3) for e, v in us.items()},
+        "escalations_total": esc,
+        "res64_mismatches": sum(not r[e]["res64_after_1000_matches_reference"] for r in rows for e in ("fp64", "ntt")),
+        "e2e": {"value": round(1e6 * walls[lead] / (iters[lead] * len(primes)), 3), "unit": "us/iteration",
+                "call": "llg_run(p, K, engine, n) per prime through the C-ABI: tables, s_0 upload, every "
+                        "attempt (escalations included), residue rebuilt on the device, result struct back",
+                "h2d_bytes_per_step": sum(4 * SWEEP_N for _ in primes), "d2h_bytes_per_step": 128 * len(primes)},
+        "clocks": clk.summary(),
+    }
+
+
+def cpu_baseline_interim(p, k0, k1, what):
+    """Reference GMP engine (oracle/_ref, compiled unchanged) per squaring at p, from
+    gmp_res64_after(p, k1) - gmp_res64_after(p, k0): one core."""
+    from oracle import oracle
+    ref = oracle.reference_module()
+    if ref is None:
+        t0 = time.perf_counter()
+        oracle.ll_gmp(p, k0)
+        t1 = time.perf_counter()
+        oracle.ll_gmp(p, k1)
+        t2 = time.perf_counter()
+        kind, call = "port", "oracle GMP restatement"
+    else:
+        t0 = time.perf_counter()
+        ref.gmp_res64_after(p, k0)
+        t1 = time.perf_counter()
+        ref.gmp_res64_after(p, k1)
+        t2 = time.perf_counter()
+        kind, call = "reference", "reference gmp_res64_after"
+    per = ((t2 - t1) - (t1 - t0)) / (k1 - k0)
+    return {"value": round(per * 1e6, 1), "unit": "us/iteration", "cores": 1, "kind": kind,
+            "sample": f"{call}(p={p}, {k1}) - ({k0}): {k1 - k0} full-size squarings of {what}"}
+
+
 def cpu_baseline_big(threads):
     """Reference CPU time per Lucas-Lehmer squaring at p = 136,279,841, from the reference's own
     squaring micro-benchmark bench_square(bits, iters, depth) (lucaslehmer.cpp:181-205; GMP mpz
@@ -438,8 +617,11 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", choices=("big", "range"), default="big")
-    ap.add_argument("--engine", choices=("fp64", "ntt"), default="fp64", help="big workload's engine")
+    ap.add_argument("--workload", choices=("big", "range", "single", "sweep"), default="big")
+    ap.add_argument("--engine", choices=("fp64", "ntt"), default="fp64",
+                    help="engine of the big workload; the reported engine of single and sweep")
+    ap.add_argument("--sweep-iters", type=int, default=100000, help="sweep: FP64 squarings timed per prime")
+    ap.add_argument("--sweep-ntt-iters", type=int, default=20000, help="sweep: NTT squarings timed per prime")
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -452,12 +634,24 @@ def main():
         vals = []
         # the reference's CPU engine keeps no state between steps: warm-up steps are not repeated
         for _ in range(args.steps):
-            vals.append(cpu_baseline_range(threads, budget_s=15.0) if args.workload == "range"
-                        else cpu_baseline_big(threads))
+            if args.workload == "range":
+                vals.append(cpu_baseline_range(threads, budget_s=15.0))
+            elif args.workload == "single":
+                vals.append(cpu_baseline_interim(SINGLE_P, 40, 2040, "a 1,257,787-bit residue"))
+            elif args.workload == "sweep":
+                vals.append(cpu_baseline_interim(22685363, 30, 130, "a 22,685,363-bit residue"))
+            else:
+                vals.append(cpu_baseline_big(threads))
         v = statistics.median(x["value"] for x in vals)
         if args.workload == "range":
             metric, unit, hib, scaling = METRIC_RANGE, "tests/s", True, "strong"
             cfg = {"workload": "range p<=100001 (9592 LL tests)"}
+        elif args.workload == "single":
+            metric, unit, hib, scaling = METRIC_SINGLE, "us/iteration", False, "weak"
+            cfg = {"workload": "p=1,257,787, one Lucas-Lehmer squaring (reference GMP engine)"}
+        elif args.workload == "sweep":
+            metric, unit, hib, scaling = METRIC_SWEEP, "us/iteration", False, "weak"
+            cfg = {"workload": "p=22,685,363 (median sweep prime), one Lucas-Lehmer squaring (reference GMP engine)"}
         else:
             metric, unit, hib, scaling = METRIC_BIG, "us/iteration", False, "weak"
             cfg = {"workload": "p=136,279,841, one Lucas-Lehmer squaring (reference GMP engine)"}
@@ -470,14 +664,18 @@ def main():
         print(json.dumps(line))
         return 0
     rank, world, local = dist_setup(args.gpus)
-    if args.workload == "range":
-        line = bench_range(args, rank, world)
-    else:
-        line = bench_big(args, rank, world)
+    bench = {"range": bench_range, "single": bench_single, "sweep": bench_sweep}.get(args.workload, bench_big)
+    line = bench(args, rank, world)
     if rank == 0:
         if not args.no_cpu_baseline and world == 1:
-            line["cpu_baseline"] = (cpu_baseline_range(threads) if args.workload == "range"
-                                    else cpu_baseline_big(threads))
+            if args.workload == "range":
+                line["cpu_baseline"] = cpu_baseline_range(threads)
+            elif args.workload == "single":
+                line["cpu_baseline"] = cpu_baseline_interim(SINGLE_P, 40, 2040, "a 1,257,787-bit residue")
+            elif args.workload == "sweep":
+                line["cpu_baseline"] = cpu_baseline_interim(22685363, 30, 130, "a 22,685,363-bit residue")
+            else:
+                line["cpu_baseline"] = cpu_baseline_big(threads)
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
