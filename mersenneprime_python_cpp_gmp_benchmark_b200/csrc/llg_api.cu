@@ -61,6 +61,7 @@ constexpr int kSmallLogMax = 13;  // N = 8192
 
 struct DeviceTables {
     std::map<uint32_t, double2*> qtw;      // quarter-wave twiddles of the M-point FFT, by M
+    std::map<uint32_t, double2*> qtw_s;    // the same in the spread layout (qpad_s), by M
     uint64_t* nqtw[kSmallLogMax + 1] = {}; // NTT: padded quarter table of the N-point transform
     NttConst nk[kSmallLogMax + 1] = {};
 };
@@ -114,12 +115,13 @@ int device_ready(int* dev_out) {
     return LLG_OK;
 }
 
-int get_qtw(int dev, uint32_t m, const double2** out) {
+int get_qtw(int dev, uint32_t m, const double2** out, bool spread = false) {
     std::lock_guard<std::mutex> lk(g_mx);
     DeviceTables& T = g_tables[dev];
-    double2*& d = T.qtw[m];
+    double2*& d = spread ? T.qtw_s[m] : T.qtw[m];
     if (!d) {
-        std::vector<double2> h = padded_quarter_table(m);  // padded layout (qpad)
+        // padded layout (qpad), or the spread one (qpad_s)
+        std::vector<double2> h = spread ? spread_quarter_table(m) : padded_quarter_table(m);
         CK(cudaMalloc(&d, h.size() * sizeof(double2)));
         CK(cudaMemcpy(d, h.data(), h.size() * sizeof(double2), cudaMemcpyHostToDevice));
     }
@@ -344,7 +346,7 @@ int launch_group(llg_batch* b, Group& g, cudaStream_t caller) {
                             (SmallResult*)g.d_results, g.st));
     } else if (is_small_pow2_length(g.n)) {
         const double2* qtw = nullptr;
-        int rc = get_qtw(b->dev, g.n / 2, &qtw);
+        int rc = get_qtw(b->dev, g.n / 2, &qtw, small_fp64_spread_table(ilog2_exact(g.n)));
         if (rc) return rc;
         float* elog = (cnt == 1) ? b->d_errlog : nullptr;
         CK(launch_small_fp64(ilog2_exact(g.n), (const SmallJob*)g.d_jobs, cnt, qtw, (int64_t*)g.d_digits,

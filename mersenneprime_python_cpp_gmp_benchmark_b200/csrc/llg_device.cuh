@@ -136,14 +136,22 @@ struct Dft<16, INV> {
 // the radix passes (multiples of 16 and of small odd numbers) spread over the shared-memory banks.
 __host__ __device__ constexpr uint32_t qpad(uint32_t r) { return r + (r >> 3); }
 __host__ __device__ constexpr uint32_t qpad_len(uint32_t qm) { return qm + (qm >> 3) + 1; }
+// The same quarter-wave table spread further, entry r at r + r/8 + r/64: the whole-test kernel's
+// twiddle reads at index n2 k1 (8 lanes of a quarter warp, strides k1 and 16 k1) and its
+// digit-reversed real-FFT twiddles then land in more of the 8 bank groups of 16-byte slots.
+__host__ __device__ constexpr uint32_t qpad_s(uint32_t r) { return r + (r >> 3) + (r >> 6); }
+__host__ __device__ constexpr uint32_t qpad_s_len(uint32_t qm) { return qm + (qm >> 3) + (qm >> 6) + 1; }
+static_assert(qpad_s(255) < qpad_s_len(256) && qpad_s(1023) < qpad_s_len(1024) && qpad_s(4095) < qpad_s_len(4096),
+              "spread quarter table length");
 
 // Twiddle e^{-2 pi i x / M} (conjugated when inv) from a padded quarter-wave table
 // q[qpad(r)] = e^{-2 pi i r / M}, r < M/4.  x in [0, M).
-template <int LOG_M>
+// SPREAD: the table is in the qpad_s layout.
+template <int LOG_M, bool SPREAD = false>
 __device__ __forceinline__ double2 twiddle(const double2* __restrict__ q, uint32_t x, bool inv) {
     constexpr uint32_t QM = (1u << LOG_M) / 4;
     const uint32_t quad = (x / QM) & 3u;
-    double2 w = q[qpad(x % QM)];
+    double2 w = q[SPREAD ? qpad_s(x % QM) : qpad(x % QM)];
     // rotate by (-i)^quad
     double2 r;
     switch (quad) {

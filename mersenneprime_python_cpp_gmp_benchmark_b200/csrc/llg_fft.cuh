@@ -17,8 +17,8 @@ namespace llg {
 
 // Twiddle table of a geometry: e^{-2 pi i r / M} at slot qpad(r) for r < M/4 (TW_QUARTER: the
 // other quadrants by rotation), r < M/2 (TW_HALF: the other half by negation), or r < M (TW_FULL:
-// one table read, no fold).
-enum { TW_QUARTER = 0, TW_HALF = 1, TW_FULL = 2 };
+// one table read, no fold); TW_QUARTER_S: the quarter table at slot qpad_s(r).
+enum { TW_QUARTER = 0, TW_HALF = 1, TW_FULL = 2, TW_QUARTER_S = 3 };
 
 // L = 2^LOG_M points, E = 2^LOG_E values per thread (radix-E passes, the last one RLAST).
 template <int LOG_M, int LOG_E = 4>
@@ -94,6 +94,8 @@ __device__ __forceinline__ double2 twiddle_g(const double2* __restrict__ q, uint
         const double2 w = q[qpad(x & (H - 1))];
         const bool ng = (x & H) != 0;  // e^{-2 pi i (r + M/2) / M} = -e^{-2 pi i r / M}
         return make_double2(ng ? -w.x : w.x, (ng != inv) ? -w.y : w.y);
+    } else if constexpr (G::TWM == TW_QUARTER_S) {
+        return twiddle<G::LOG_M_, true>(q, x, inv);
     } else {
         return twiddle<G::LOG_M_>(q, x, inv);
     }
@@ -203,6 +205,7 @@ struct SmallG : SmallGeom<LOG_M_T, LOG_E> {
 // Length (16-byte slots) of the twiddle table a geometry reads.
 template <class G>
 __host__ __device__ constexpr uint32_t twiddle_table_len() {
+    if (G::TWM == TW_QUARTER_S) return qpad_s_len((uint32_t)G::M >> 2);
     return qpad_len((uint32_t)G::M >> (G::TWM == TW_FULL ? 0 : G::TWM == TW_HALF ? 1 : 2));
 }
 

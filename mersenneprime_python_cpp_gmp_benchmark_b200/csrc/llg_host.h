@@ -22,6 +22,8 @@ std::vector<int> seed_digits(uint64_t n);
 std::vector<double2> padded_quarter_table(uint64_t L);
 // Value of slot i of that layout (zero in the padding slots).
 double2 padded_quarter_slot(uint64_t L, uint64_t i);
+// The same quarter-wave table in the spread layout (entry r at qpad_s(r)).
+std::vector<double2> spread_quarter_table(uint64_t L);
 
 struct LargeTest {
     uint64_t p = 0, M = 0;

@@ -62,6 +62,14 @@ double2 padded_quarter_slot(uint64_t L, uint64_t i) {
     return make_double2((double)cosl(ang), -(double)sinl(ang));
 }
 
+std::vector<double2> spread_quarter_table(uint64_t L) {
+    const uint32_t qm = (uint32_t)(L / 4);
+    std::vector<double2> t(qpad_s_len(qm), make_double2(0.0, 0.0));
+    // entry r holds the value slot qpad(r) holds in the padded layout (the same long-double sum)
+    for (uint32_t r = 0; r < qm; ++r) t[qpad_s(r)] = padded_quarter_slot(L, qpad(r));
+    return t;
+}
+
 std::vector<double2> padded_quarter_table(uint64_t L) {
     const uint64_t n = qpad_len((uint32_t)(L / 4));
     std::vector<double2> t(n);

@@ -36,8 +36,13 @@ namespace llg {
 // log2 of the complex values per thread for M = 2^log_m: 8 (radix-8 passes, twice the warps)
 // for M = 2^9, where that takes no more passes than 16 (8 x 8 x 8 against 16 x 16 x 2); 16 else
 __host__ __device__ constexpr int small_log_e(int log_m) { return log_m == 9 ? 3 : 4; }
+// twiddle-table layout: spread (qpad_s) from M = 2^10 up, where the radix-16 passes' strided
+// reads and the real-FFT split's digit-reversed reads conflict most in the qpad layout
+__host__ __device__ constexpr int small_tw_layout(int log_m) { return log_m >= 10 ? TW_QUARTER_S : TW_QUARTER; }
 template <int LOG_M>
-using SmallGeo = SmallG<LOG_M, small_log_e(LOG_M), TW_QUARTER>;
+using SmallGeo = SmallG<LOG_M, small_log_e(LOG_M), small_tw_layout(LOG_M)>;
+
+bool small_fp64_spread_table(int log_n) { return small_tw_layout(log_n - 1) == TW_QUARTER_S; }
 // blocks per SM the kernel is built for: 128 registers a thread at 16 values, ~85 at 8
 __host__ __device__ constexpr int small_min_blocks(int t, int le) {
     return t < 32 ? 16 : (le >= 4 ? 512 : 768) / t > 16 ? 16 : (le >= 4 ? 512 : 768) / t;
