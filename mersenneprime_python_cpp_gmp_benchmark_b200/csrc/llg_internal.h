@@ -25,10 +25,10 @@ struct SmallResult {
     uint32_t pad;
 };
 
-// FP64 whole-test kernel, N = 2^log_n with 5 <= log_n <= 13. digits: njobs * N int64 (may be null).
 // Whether the whole-test FP64 kernel of length 2^log_n reads its twiddle table in the spread
 // layout (spread_quarter_table) rather than the padded one (padded_quarter_table).
 bool small_fp64_spread_table(int log_n);
+// FP64 whole-test kernel, N = 2^log_n with 5 <= log_n <= 13. digits: njobs * N int64 (may be null).
 cudaError_t launch_small_fp64(int log_n, const SmallJob* jobs, int njobs, const double2* qtw,
                               int64_t* digits, SmallResult* results, float* errlog,
                               double abort_err, cudaStream_t st);
