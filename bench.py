@@ -8,7 +8,9 @@ Workloads (synthetic inputs: the exponents themselves, s_0 = 4; no dataset exist
           squarings. metric: us per Lucas-Lehmer iteration (lower is better). value: CUDA events on
           the launch stream, the 64 MiB state resident on the device, L2 flushed between steps.
           e2e: lucaslehmer.fft_res64_after(p, 2000) -- tables, upload of s_0, squarings, exact
-          residue rebuilt on the device, res64 back -- per squaring.
+          residue rebuilt on the device, res64 back -- per squaring. The line also carries the
+          other half of the metric as "range" (the range workload below, one timed step; leave it
+          out with --no-range).
   range   every prime p <= 100,001 (9,592 Lucas-Lehmer tests, 28 Mersenne hits), batched whole-test
           kernels bucketed by transform length. One step = every test run to completion.
           metric: tests/s. e2e: lucaslehmer_cuda.lucas_lehmer_batch() on the host list.
@@ -19,9 +21,11 @@ Workloads (synthetic inputs: the exponents themselves, s_0 = 4; no dataset exist
           final residue zero, the round-off maximum and per-squaring log.
   sweep   8 seeded primes in [20M, 25M]: FP64 asked at N = 2^20 (escalating on round-off > 0.4)
           against the NTT at its exact length; length used, escalations, round-off, us per squaring.
---impl reference: the reference's own CPU engine (its lucaslehmer.cpp compiled unchanged into
-oracle/_ref/) on the host cores for the same metric: bench_square at p = 136,279,841 (big) or a
-stratified sample of the range (range).
+--impl reference: the reference's own CPU engines (its lucaslehmer.cpp compiled unchanged into
+oracle/_ref/) on the host cores for the same metric: bench_square at p = 136,279,841 (big; with
+the range sample beside it) or a stratified sample of the range (range), GMP engine as the value
+and FFT engine beside it. FFTW3 is absent, so the reference FFT engine runs over the oracle's
+radix-2 FFT; its published FFTW figure for the range is quoted with it.
 """
 from __future__ import annotations
 
@@ -49,8 +53,8 @@ STEP_ITERS = 1000  # squarings per timed step of the p=136,279,841 workload
 PASS_ITERS = 100   # squarings timed pass by pass for the dominant kernel's roofline
 # DRAM bytes (read + write) of one launch at p=136,279,841, N=2^23, from an ncu capture of
 # `python -m mersenneprime_python_cpp_gmp_benchmark_b200.llgpu square --p 136279841 --n 8388608
-# --iters 6 --shape 10,8` (the autotuned shape; NTT: `... --iters 6 --engine ntt`;
-# profiles/two_pass_p136279841.md). The 64 MiB state is partly L2-resident between the passes.
+# --iters 6` (NTT: `... --iters 6 --engine ntt`). ncu captures run cold (caches flushed), so these
+# are upper bounds on a warm launch, where part of the 64 MiB state is still in L2.
 NCU_TRAFFIC = {"fp64": {"row": 106451200, "column": 78296064},
                "ntt": {"row": 115433728, "column": 94066176}}
 
@@ -586,30 +590,78 @@ def cpu_baseline_big(threads):
                       "Karatsuba split), the mod 2^p-1 shift-and-add (~1% of a squaring) not included"}
 
 
-def cpu_baseline_range(threads, budget_s=20.0):
-    """Reference GMP engine (oracle/_ref, compiled unchanged) on a stratified sample of the range."""
-    from oracle import oracle
-    ref = oracle.reference_module()
-    kind = "reference"
-    if ref is None:
-        kind = "port"
+# Published wall time of the reference's FFT engine (FFTW3) over every prime p <= 100001 on a Xeon
+# w5-3435X with 32 threads (reference README.md:96,127-128): the yardstick of the range target.
+PUBLISHED_FFT_RANGE = {"wall_s": 442.5, "threads": 32, "host": "Xeon w5-3435X (16C/32T)",
+                       "tests_per_s": round(9592 / 442.5, 2), "source": "reference README.md:96,127-128"}
+
+
+def _range_sample(threads, budget_s, cost_per_1e5):
+    """Every k-th prime p <= 100001 (offset k/2), k the smallest power of two >= 64 whose sample
+    fits the budget on `threads` threads (a test's cost grows as ~p^2.3)."""
     ps = sieve(2, RANGE_HI)
-    # stratified: every k-th prime; grow k until the sample fits the budget (cost ~ p^2.3)
     k = 64
-    est = lambda kk: sum((p / 1e5) ** 2.3 * 9.0 for p in ps[::kk]) / threads  # ~9 s per p=1e5 test
+    est = lambda kk: sum((p / 1e5) ** 2.3 * cost_per_1e5 for p in ps[::kk]) / threads
     while est(k) > budget_s and k < 4096:
         k *= 2
-    sample = ps[k // 2::k]
-    run = (lambda p: ref.lucas_lehmer_res(p)) if ref else (lambda p: oracle.ll_gmp(p)[:2])
+    return ps, k, ps[k // 2::k]
+
+
+def _time_sample(run, sample, threads):
     t0 = time.perf_counter()
     with ThreadPoolExecutor(threads) as ex:
         list(ex.map(run, sorted(sample, reverse=True)))
-    wall = time.perf_counter() - t0
-    est_wall = wall * k
-    return {"value": round(len(ps) / est_wall, 4), "unit": "tests/s", "cores": threads, "kind": kind,
-            "sample": f"reference GMP engine (lucaslehmer_res) on every {k}th prime p<=100001 "
-                      f"({len(sample)} tests, {wall:.1f} s wall on {threads} threads); full-range wall "
-                      f"extrapolated as sample wall x {k}"}
+    return time.perf_counter() - t0
+
+
+def cpu_baseline_range(threads, budget_s=20.0):
+    """The reference's CPU engines (oracle/_ref: its lucaslehmer.cpp compiled unchanged) on a
+    stratified sample of the range, all host threads: the GMP engine (lucas_lehmer_res,
+    lucaslehmer.cpp:29-58) as the reported value, and the FFT engine (lucas_lehmer_fft_res,
+    lucaslehmer.cpp:257-335) beside it. FFTW3 is not installed, so the FFT engine runs its own
+    code over the oracle's radix-2 FFT behind FFTW's plan API, several times slower than FFTW;
+    the published FFTW figure is quoted next to it."""
+    from oracle import oracle
+    ref = oracle.reference_module()
+    kind = "reference" if ref else "port"
+    ps, k, sample = _range_sample(threads, budget_s, 9.0)
+    run = (lambda p: ref.lucas_lehmer_res(p)) if ref else (lambda p: oracle.ll_gmp(p)[:2])
+    wall = _time_sample(run, sample, threads)
+    out = {"value": round(len(ps) / (wall * k), 4), "unit": "tests/s", "cores": threads, "kind": kind,
+           "sample": f"reference GMP engine (lucas_lehmer_res) on every {k}th prime p<=100001 "
+                     f"({len(sample)} tests, {wall:.1f} s wall on {threads} threads); full-range wall "
+                     f"extrapolated as sample wall x {k}"}
+    if ref:
+        ps, kf, fs = _range_sample(threads, budget_s, 25.0)
+        wf = _time_sample(lambda p: ref.lucas_lehmer_fft_res(p), fs, threads)
+        out["fft_engine"] = {
+            "value": round(len(ps) / (wf * kf), 4), "unit": "tests/s", "cores": threads,
+            "kind": "reference code over a substitute FFT",
+            "sample": f"reference FFT engine (lucas_lehmer_fft_res) on every {kf}th prime p<=100001 "
+                      f"({len(fs)} tests, {wf:.1f} s wall on {threads} threads), extrapolated x {kf}; "
+                      "FFTW3 is absent, so its FFT calls run the oracle's radix-2 FFT (not FFTW)"}
+    out["fft_engine_published"] = PUBLISHED_FFT_RANGE
+    return out
+
+
+def cpu_baseline_big_fft():
+    """The reference's FFT engine (oracle/_ref) per squaring at p = 136,279,841, N = 2^23:
+    fft_res64_after(p, 3) - fft_res64_after(p, 1), one thread, over the substitute FFT."""
+    from oracle import oracle
+    ref = oracle.reference_module()
+    if ref is None:
+        return None
+    ref.fft_res64_after(1257787, 2)  # planning and table paths warmed
+    t0 = time.perf_counter()
+    ref.fft_res64_after(BIG_P, 1)
+    t1 = time.perf_counter()
+    ref.fft_res64_after(BIG_P, 3)
+    t2 = time.perf_counter()
+    per = ((t2 - t1) - (t1 - t0)) / 2.0
+    return {"value": round(per * 1e6, 1), "unit": "us/iteration", "cores": 1,
+            "kind": "reference code over a substitute FFT",
+            "sample": "reference fft_res64_after(136279841, 3) - (136279841, 1): 2 squarings at N = 8,388,608; "
+                      "FFTW3 is absent, so its FFT calls run the oracle's radix-2 FFT (not FFTW)"}
 
 
 def main():
@@ -624,6 +676,8 @@ def main():
     ap.add_argument("--sweep-ntt-iters", type=int, default=20000, help="sweep: NTT squarings timed per prime")
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-range", action="store_true",
+                    help="big: leave out the range sub-record (the other half of the metric)")
     args = ap.parse_args()
     threads = os.cpu_count() or 1
     if args.impl == "reference":
@@ -643,6 +697,11 @@ def main():
             else:
                 vals.append(cpu_baseline_big(threads))
         v = statistics.median(x["value"] for x in vals)
+        extra = {}
+        if args.workload == "big":
+            vals[-1]["fft_engine"] = cpu_baseline_big_fft()
+            if not args.no_range:  # the other half of the metric, sampled once
+                extra["range"] = cpu_baseline_range(threads, budget_s=15.0)
         if args.workload == "range":
             metric, unit, hib, scaling = METRIC_RANGE, "tests/s", True, "strong"
             cfg = {"workload": "range p<=100001 (9592 LL tests)"}
@@ -661,11 +720,16 @@ def main():
                 "config": cfg, "impl": "reference", "cpu_baseline": vals[-1],
                 "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                 "ms_per_step": round(1e3 * (time.perf_counter() - t0) / max(1, args.steps), 1)}
+        line.update(extra)
         print(json.dumps(line))
         return 0
     rank, world, local = dist_setup(args.gpus)
     bench = {"range": bench_range, "single": bench_single, "sweep": bench_sweep}.get(args.workload, bench_big)
     line = bench(args, rank, world)
+    rng = None
+    if args.workload == "big" and not args.no_range:
+        # the other half of the metric: every prime p <= 100001, one timed step after one warm-up
+        rng = bench_range(argparse.Namespace(**{**vars(args), "steps": 1, "warmup": 1}), rank, world)
     if rank == 0:
         if not args.no_cpu_baseline and world == 1:
             if args.workload == "range":
@@ -676,6 +740,13 @@ def main():
                 line["cpu_baseline"] = cpu_baseline_interim(22685363, 30, 130, "a 22,685,363-bit residue")
             else:
                 line["cpu_baseline"] = cpu_baseline_big(threads)
+                line["cpu_baseline"]["fft_engine"] = cpu_baseline_big_fft()
+                if rng is not None:
+                    rng["cpu_baseline"] = cpu_baseline_range(threads)
+        if rng is not None:
+            for k in ("n_gpus", "steps", "warmup", "higher_is_better", "scaling", "vs_baseline", "dtype"):
+                rng.pop(k, None)
+            line["range"] = rng
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist

@@ -164,7 +164,10 @@ int llg_residue_from_digits_device(uint64_t p, uint32_t n, const int32_t* d_digi
  * default stream) and returns when it has finished; LLG_E_ROUNDOFF if the round-off exceeded 0.4.
  * Every call reuses the same array and leaves its contents behind; the call zeroes what has to
  * start at zero. Calls whose GPU work overlaps race on the array: serialise them. The first call
- * on each device looks up the array's device address; make it outside any stream capture. */
+ * on each device looks up the array's device address. Every call uploads its tables with a
+ * host-synchronous copy (skipped when p and n repeat the previous call's) and waits for `stream`,
+ * so no call may be made while `stream` is being captured. A failure after work was enqueued
+ * waits for `stream` too, so the array is idle when the call returns. */
 #define LLG_NOALLOC_MAX_N 65536u
 #define LLG_NOALLOC_SCRATCH_BYTES (640u * 1024u)
 int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* digits_out, double* max_err,

@@ -3,9 +3,29 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 
 namespace llg {
+
+// Per-device record of a one-time kernel setup (cudaFuncSetAttribute applies to the current device
+// only): done() for the current device, mark() after the setup succeeded there. Devices 0..63; the
+// race between two first launches is benign (the setup is idempotent).
+struct PerDeviceOnce {
+    std::atomic<unsigned long long> bits{0};
+    static int current() {
+        int d = 0;
+        return cudaGetDevice(&d) == cudaSuccess && d >= 0 && d < 64 ? d : -1;
+    }
+    bool done() const {
+        const int d = current();
+        return d >= 0 && ((bits.load() >> d) & 1ull);
+    }
+    void mark() {
+        const int d = current();
+        if (d >= 0) bits.fetch_or(1ull << d);
+    }
+};
 
 enum : uint32_t {
     LLG_ST_OK = 0,

@@ -16,8 +16,11 @@
 //     what must start at zero (the control block) and overwrites everything else before reading
 //     it. Two calls whose GPU work overlaps (different streams, or different host threads) race on
 //     the array and produce wrong results: serialise them.
-//   * The first call on each device looks up the array's device address (cudaGetSymbolAddress);
-//     make that first call outside any stream capture.
+//   * The first call on each device looks up the array's device address (cudaGetSymbolAddress).
+//     Every call uploads its tables with a host-synchronous copy and waits for `stream` before it
+//     returns, so no call may be made while `stream` is being captured into a CUDA graph.
+//   * On an error after the first enqueue the call waits for `stream` before it returns, so the
+//     array is idle again when the next call starts.
 //   * The caller passes the output: digits_out, a device buffer of N int32 values, receives the
 //     balanced digits of s_iters in natural order (llg_residue_from_digits turns them into the
 //     residue). The call enqueues on `stream` (NULL: the legacy default stream) and returns after
@@ -26,6 +29,7 @@
 
 #include <cmath>
 #include <cstddef>
+#include <cstdio>
 #include <cstring>
 #include <mutex>
 
@@ -49,9 +53,16 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 std::mutex g_noalloc_mx;
 unsigned char* g_scratch_addr[kMaxDevices] = {};
 
-// Host staging for the tables (no host allocation either): the largest table set is ~24 KiB.
+// Host staging for the tables (no host allocation either): the largest table set is ~24 KiB. The
+// tables are laid out contiguously in the array (qtwC .. sB), so one copy moves all of them.
 constexpr size_t kStageBytes = 64u * 1024u;
-alignas(64) unsigned char g_stage[kStageBytes];
+alignas(256) unsigned char g_stage[kStageBytes];
+// (p, n) whose tables the array holds, per device: a repeated call skips the upload
+struct TableKey {
+    uint64_t p = 0;
+    uint32_t n = 0;
+};
+TableKey g_tables_for[kMaxDevices];
 
 struct Layout {
     size_t V, carry, carry2, halo, ctl, flags, qtwC, qtwR, tw1, tw2, pos_of_c, wA, iwA, sA, wB, iwB, sB, end;
@@ -100,23 +111,17 @@ int pos_of_freq_host(int log_l, int k) {
     return rest * RLAST + klast;
 }
 
-// Copies `count` table entries produced by f(i) into the scratch at byte offset `off`, through
-// the static host stage in slices.
+// Writes `count` table entries produced by f(i) into the host stage at byte offset `off`.
 template <class T, class F>
-cudaError_t put_table(unsigned char* dev, size_t off, size_t count, F f, cudaStream_t st) {
-    T* stage = reinterpret_cast<T*>(g_stage);
-    const size_t per = kStageBytes / sizeof(T);
-    for (size_t base = 0; base < count; base += per) {
-        const size_t n = count - base < per ? count - base : per;
-        for (size_t i = 0; i < n; ++i) stage[i] = f(base + i);
-        // pageable source: the copy has consumed the stage when the call returns
-        cudaError_t e = cudaMemcpyAsync(dev + off + base * sizeof(T), stage, n * sizeof(T),
-                                        cudaMemcpyHostToDevice, st);
-        if (e != cudaSuccess) return e;
-        e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) return e;
-    }
-    return cudaSuccess;
+void stage_table(size_t off, size_t count, F f) {
+    T* dst = reinterpret_cast<T*>(g_stage + off);
+    for (size_t i = 0; i < count; ++i) dst[i] = f(i);
+}
+
+int cuda_fail(const char* what, cudaError_t e) {
+    char msg[256];
+    snprintf(msg, sizeof msg, "llg_run_noalloc: %s: %s", what, cudaGetErrorString(e));
+    return set_error(e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ? LLG_E_NODEV : LLG_E_CUDA, msg);
 }
 
 double2 omega(uint64_t period, uint64_t e) {
@@ -153,41 +158,54 @@ extern "C" int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* 
     const Layout L = layout(logN, logC, logR, s);
     if (L.end > kNoAllocScratchBytes) return set_error(LLG_E_UNSUPPORTED, "llg_run_noalloc: state exceeds the array");
 
+    if (L.end - L.qtwC > kStageBytes) return set_error(LLG_E_UNSUPPORTED, "llg_run_noalloc: tables exceed the host stage");
+
     std::lock_guard<std::mutex> lk(g_noalloc_mx);
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return LLG_E_NODEV;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail("no current device", e);
+    if (dev < 0 || dev >= kMaxDevices) return set_error(LLG_E_NODEV, "llg_run_noalloc: device ordinal out of range");
     if (!g_scratch_addr[dev]) {
         void* ptr = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-        if (e != cudaSuccess || !ptr) return LLG_E_CUDA;
+        e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr) return cuda_fail("looking up the array's device address", e);
         g_scratch_addr[dev] = static_cast<unsigned char*>(ptr);
     }
     unsigned char* base = g_scratch_addr[dev];
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    cudaError_t e = configure_large(logC, large_rows_per_block(logC), logR);
-    if (e != cudaSuccess) return LLG_E_CUDA;
+    e = configure_large(logC, large_rows_per_block(logC), logR);
+    if (e != cudaSuccess) return cuda_fail("configuring the kernels", e);
 
-    // tables (exact integers and long-double rounded values, as the allocating path uses)
-    const long double Nl = (long double)N;
-#define PUT(T, off, cnt, expr)                                                          \
-    do {                                                                                \
-        e = put_table<T>(base, off, cnt, [&](size_t i) -> T { return expr; }, st);      \
-        if (e != cudaSuccess) return LLG_E_CUDA;                                        \
-    } while (0)
-    PUT(double2, L.qtwC, (size_t)qpad_len((uint32_t)C), padded_quarter_slot(C, i));
-    PUT(double2, L.qtwR, (size_t)qpad_len((uint32_t)R / 4), padded_quarter_slot(R, i));
-    PUT(double2, L.tw1, (size_t)1 << s, omega(M, i));
-    PUT(double2, L.tw2, (size_t)(M >> s), omega(M, (uint64_t)i << s));
-    PUT(int, L.pos_of_c, (size_t)C, pos_of_freq_host(logC, (int)i));
-    auto sAj = [&](size_t j) { return (N - (uint64_t)(((unsigned __int128)j * p) % N)) % N; };
-    auto sBb = [&](size_t b) { return (N - (uint64_t)(((unsigned __int128)2 * R * b * p) % N)) % N; };
-    PUT(double, L.wA, (size_t)2 * R, (double)exp2l((long double)sAj(i) / Nl));
-    PUT(double, L.iwA, (size_t)2 * R, (double)exp2l(-(long double)sAj(i) / Nl));
-    PUT(int, L.sA, (size_t)2 * R, (int)sAj(i));
-    PUT(double, L.wB, (size_t)C, (double)exp2l((long double)sBb(i) / Nl));
-    PUT(double, L.iwB, (size_t)C, (double)(exp2l(-(long double)sBb(i) / Nl) / (4.0L * (long double)M)));
-    PUT(int, L.sB, (size_t)C, (int)sBb(i));
-#undef PUT
+    // tables (exact integers and long-double rounded values, as the allocating path uses), built
+    // in the host stage at their offsets in the array and uploaded in one copy
+    if (g_tables_for[dev].p != p || g_tables_for[dev].n != n) {
+        g_tables_for[dev] = TableKey{};  // invalid until the upload below has completed
+        const long double Nl = (long double)N;
+        const size_t o = L.qtwC;
+        std::memset(g_stage, 0, L.end - o);
+        stage_table<double2>(L.qtwC - o, qpad_len((uint32_t)C), [&](size_t i) { return padded_quarter_slot(C, i); });
+        stage_table<double2>(L.qtwR - o, qpad_len((uint32_t)R / 4), [&](size_t i) { return padded_quarter_slot(R, i); });
+        stage_table<double2>(L.tw1 - o, (size_t)1 << s, [&](size_t i) { return omega(M, i); });
+        stage_table<double2>(L.tw2 - o, (size_t)(M >> s), [&](size_t i) { return omega(M, (uint64_t)i << s); });
+        stage_table<int>(L.pos_of_c - o, (size_t)C, [&](size_t i) { return pos_of_freq_host(logC, (int)i); });
+        auto sAj = [&](size_t j) { return (N - (uint64_t)(((unsigned __int128)j * p) % N)) % N; };
+        auto sBb = [&](size_t b) { return (N - (uint64_t)(((unsigned __int128)2 * R * b * p) % N)) % N; };
+        stage_table<double>(L.wA - o, (size_t)2 * R, [&](size_t i) { return (double)exp2l((long double)sAj(i) / Nl); });
+        stage_table<double>(L.iwA - o, (size_t)2 * R, [&](size_t i) { return (double)exp2l(-(long double)sAj(i) / Nl); });
+        stage_table<int>(L.sA - o, (size_t)2 * R, [&](size_t i) { return (int)sAj(i); });
+        stage_table<double>(L.wB - o, (size_t)C, [&](size_t i) { return (double)exp2l((long double)sBb(i) / Nl); });
+        stage_table<double>(L.iwB - o, (size_t)C,
+                            [&](size_t i) { return (double)(exp2l(-(long double)sBb(i) / Nl) / (4.0L * (long double)M)); });
+        stage_table<int>(L.sB - o, (size_t)C, [&](size_t i) { return (int)sBb(i); });
+        // pageable source: the copy has consumed the stage once the stream has finished it
+        e = cudaMemcpyAsync(base + o, g_stage, L.end - o, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            cudaStreamSynchronize(st);
+            return cuda_fail("uploading the tables", e);
+        }
+        g_tables_for[dev] = TableKey{p, n};
+    }
 
     LargeArgs A;
     std::memset(&A, 0, sizeof A);
@@ -220,27 +238,36 @@ extern "C" int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* 
     A.rem = (int)(p & (N - 1));
     A.logN = logN;
 
-    // s_0 = 4 as digits (the output buffer doubles as the INIT input), control block cleared
+    // s_0 = 4 as digits (the output buffer doubles as the INIT input), control block cleared.
+    // From the first enqueue on, a failure waits for the stream before returning.
+    auto fail_enqueued = [&](const char* what, cudaError_t err) {
+        cudaStreamSynchronize(st);
+        return cuda_fail(what, err);
+    };
     static const int32_t four = 4;
-    if (cudaMemsetAsync(digits_out, 0, N * sizeof(int32_t), st) != cudaSuccess) return LLG_E_CUDA;
-    if (cudaMemcpyAsync(digits_out, &four, sizeof four, cudaMemcpyHostToDevice, st) != cudaSuccess)
-        return LLG_E_CUDA;
-    if (cudaMemsetAsync(A.ctl, 0, sizeof(LargeCtl), st) != cudaSuccess) return LLG_E_CUDA;
-    if (cudaMemsetAsync(A.flags, 0, (size_t)A.nblocks * sizeof(unsigned), st) != cudaSuccess) return LLG_E_CUDA;
-    if (launch_large_row(logC, large_rows_per_block(logC), LARGE_INIT, A, st) != cudaSuccess) return LLG_E_CUDA;
-    if (launch_large_col(logR, A, st) != cudaSuccess) return LLG_E_CUDA;
+    if ((e = cudaMemsetAsync(digits_out, 0, N * sizeof(int32_t), st)) != cudaSuccess)
+        return fail_enqueued("clearing digits_out", e);
+    if ((e = cudaMemcpyAsync(digits_out, &four, sizeof four, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return fail_enqueued("writing s_0", e);
+    if ((e = cudaMemsetAsync(A.ctl, 0, sizeof(LargeCtl), st)) != cudaSuccess) return fail_enqueued("clearing the control block", e);
+    if ((e = cudaMemsetAsync(A.flags, 0, (size_t)A.nblocks * sizeof(unsigned), st)) != cudaSuccess)
+        return fail_enqueued("clearing the carry flags", e);
+    const int G = large_rows_per_block(logC);
+    if ((e = launch_large_row(logC, G, LARGE_INIT, A, st)) != cudaSuccess) return fail_enqueued("row pass launch", e);
+    if ((e = launch_large_col(logR, A, st)) != cudaSuccess) return fail_enqueued("column pass launch", e);
     for (uint64_t k = 1; k < iters; ++k) {
-        if (launch_large_row(logC, large_rows_per_block(logC), LARGE_ITER, A, st) != cudaSuccess) return LLG_E_CUDA;
-        if (launch_large_col(logR, A, st) != cudaSuccess) return LLG_E_CUDA;
+        if ((e = launch_large_row(logC, G, LARGE_ITER, A, st)) != cudaSuccess) return fail_enqueued("row pass launch", e);
+        if ((e = launch_large_col(logR, A, st)) != cudaSuccess) return fail_enqueued("column pass launch", e);
     }
-    if (launch_large_row(logC, large_rows_per_block(logC), LARGE_FINAL, A, st) != cudaSuccess) return LLG_E_CUDA;
+    if ((e = launch_large_row(logC, G, LARGE_FINAL, A, st)) != cudaSuccess) return fail_enqueued("row pass launch", e);
     LargeCtl h;
-    if (cudaMemcpyAsync(&h, A.ctl, sizeof(LargeCtl), cudaMemcpyDeviceToHost, st) != cudaSuccess)
-        return LLG_E_CUDA;
-    if (cudaStreamSynchronize(st) != cudaSuccess) return LLG_E_CUDA;
+    if ((e = cudaMemcpyAsync(&h, A.ctl, sizeof(LargeCtl), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return fail_enqueued("reading the control block", e);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail("running the squarings", e);
     double err;
     std::memcpy(&err, &h.err_max, sizeof err);
     if (max_err) *max_err = err;
-    if (h.timeout) return LLG_E_TIMEOUT;
-    return err > 0.4 ? LLG_E_ROUNDOFF : LLG_OK;
+    if (h.timeout) return set_error(LLG_E_TIMEOUT, "llg_run_noalloc: a carry wait timed out");
+    if (err > 0.4) return set_error(LLG_E_ROUNDOFF, "llg_run_noalloc: round-off above 0.4 at this length");
+    return LLG_OK;
 }

@@ -352,12 +352,12 @@ static cudaError_t launch_small_t(const SmallJob* jobs, int njobs, const double2
                                   double abort_err, cudaStream_t st) {
     using G = SmallGeo<LOG_M>;
     const size_t smem = small_smem_bytes<LOG_M>();
-    static bool configured = false;  // benign race: the attribute call is idempotent
-    if (!configured) {
+    static PerDeviceOnce configured;
+    if (!configured.done()) {
         cudaError_t e = cudaFuncSetAttribute(ll_small_fp64<LOG_M>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        configured = true;
+        configured.mark();
     }
     ll_small_fp64<LOG_M><<<njobs, G::T, smem, st>>>(jobs, qtw, digits, results, errlog, abort_err);
     return cudaGetLastError();

@@ -317,12 +317,12 @@ static cudaError_t launch_mixed_t(const SmallJob* jobs, int njobs, const double2
                                   int64_t* digits, SmallResult* results, float* errlog, double abort_err,
                                   cudaStream_t st) {
     const size_t smem = mixed_smem_bytes<R0, LOG_L>();
-    static bool configured = false;  // benign race: the attribute call is idempotent
-    if (!configured) {
+    static PerDeviceOnce configured;
+    if (!configured.done()) {
         cudaError_t e = cudaFuncSetAttribute(ll_small_fp64_mixed<R0, LOG_L>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        configured = true;
+        configured.mark();
     }
     ll_small_fp64_mixed<R0, LOG_L><<<njobs, MixedGeom<R0, LOG_L>::T, smem, st>>>(jobs, qtwL, qtwM, digits,
                                                                                 results, errlog, abort_err);

@@ -17,8 +17,9 @@ def _residue_via_noalloc(gpu, torch, p, k, n):
 
 def test_noalloc_matches_allocating_entry_point(gpu):
     torch = pytest.importorskip("torch")
-    cases = [(1257787, 1000, 65536), (300007, 257, 16384)]
-    for p, k, n in cases:  # two calls in a row, different sizes: no state may leak between them
+    # N = 65536 (rows of 2^8), 32768 (rows of 2^7), 16384 (rows of 2^6): each split of the array
+    cases = [(1257787, 1000, 65536), (600011, 300, 32768), (300007, 257, 16384), (300007, 100, 16384)]
+    for p, k, n in cases:  # calls in a row, different sizes, then a repeat: no state may leak between them
         want = gpu.run(p, iters=k, n=n, want_words=True)
         (z, r64, words), err = _residue_via_noalloc(gpu, torch, p, k, n)
         assert words == want["words"] and r64 == want["res64"], (p, k, n)
