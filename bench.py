@@ -244,8 +244,10 @@ def bench_range(args, rank, world):
     assert sorted(p for p, r, s, res64 in out if r) == hits
     t_e2e = max_over_ranks(t_e2e, world)
     e2e = sum_over_ranks(len(mine), world) / t_e2e
+    # up: the job list (p, iterations) per test; back: its result record, res64 and zero flag (the
+    # residue is rebuilt on the device)
     h2d = 16 * len(mine)
-    d2h = sum(8 * r["n"] + 32 for r in res)
+    d2h = (32 + 8 + 4) * len(mine)
     flops = range_flops(res)
     achieved = flops / (t_rank / args.steps) / 1e12
     peak = llgpu.measure_peak("fp64") / 1e12

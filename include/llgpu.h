@@ -66,6 +66,11 @@ uint32_t llg_fft_length(uint64_t p, double max_bpw);
  * Replaces set_fft_bits_per_word(), lucaslehmer.cpp:368 (g_max_bpw, lucaslehmer.cpp:246). */
 int llg_set_max_bpw(double bpw);
 double llg_get_max_bpw(void);
+/* Round-off bound of the FP64 engine (default 0.4, in (0, 0.5)): a test whose worst
+ * |x - round(x)| exceeds it is redone at a longer length (two-pass lengths: from the residue of
+ * the last check that stayed within it). Replaces the fixed 0.35 bound of lucaslehmer.cpp:296. */
+int llg_set_roundoff_limit(double limit);
+double llg_get_roundoff_limit(void);
 /* NTT length for p (exactness bound ceil(p/N) <= (63 - log2 N)/2); 0 = cannot take.
  * Replaces ntt_length(), cuda/ll_ntt.cu:172-180. */
 uint32_t llg_ntt_length(uint64_t p);
@@ -132,6 +137,18 @@ int llg_test_start(llg_test* t, void* stream);
 int llg_test_iterate(llg_test* t, uint64_t iters, void* stream);
 int llg_test_read(llg_test* t, void* stream, llg_result* out, uint64_t* words, size_t nwords);
 int llg_test_errlog(llg_test* t, float* log, size_t cap, size_t* len);
+/* Sets the test's state to a residue s (ceil(p/64) little-endian limbs, s < 2^p) reached after
+ * `iters_done` squarings and starts the next squaring, as llg_test_start does from s_0 = 4. The
+ * digits are formed on the GPU at the test's own length, so a residue from any length (or from
+ * another engine) resumes here; llg_test_read's words are such a residue. Replaces restarting
+ * lucas_lehmer_fft_raw() from s_0 (lucaslehmer.cpp:272-273) after a round-off abort
+ * (lucaslehmer.cpp:296, 334): a test moved to a longer length goes on from its last residue. */
+int llg_test_load(llg_test* t, const uint64_t* words, size_t nwords, uint64_t iters_done, void* stream);
+/* Diagnostic of the bounded waits (FP64 engine): one row pass whose wrap-around job is withheld
+ * and whose flag waits give up after spin_limit sleeps of ~64 ns. Tile 0 and the last tile wait
+ * for that job's flag, give up, and the kernel returns; the call then reports LLG_E_TIMEOUT.
+ * The test's state is invalid afterwards (destroy it). No reference counterpart. */
+int llg_test_diag_withhold_wrap(llg_test* t, uint64_t spin_limit, void* stream);
 /* `iters` more squarings launched one pass at a time with CUDA events between the launches (no
  * graph): the mean device time in microseconds of the row pass and of the column pass. Waits. */
 int llg_test_time_passes(llg_test* t, uint64_t iters, void* stream, double* row_us, double* col_us);

@@ -15,6 +15,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/llgpu.h"
@@ -52,7 +53,9 @@ int fail(int code, const char* fmt, ...) {
 
 double g_max_bpw = 18.0;  // lucaslehmer.cpp:246
 std::mutex g_mx;
-const double kAbortErr = 0.4;
+// Round-off bound: a test whose worst |x - round(x)| exceeds it is redone at a longer length (the
+// reference's bound is 0.35 with a GMP redo, lucaslehmer.cpp:296; llg_set_roundoff_limit).
+std::atomic<double> g_abort_err{0.4};
 
 constexpr int kSmallLogMin = 5;   // N = 32
 constexpr int kSmallLogMax = 13;  // N = 8192
@@ -259,6 +262,13 @@ struct Group {
     void* d_jobs = nullptr;
     void* d_results = nullptr;  // SmallResult[] or uint64_t[] (word path)
     void* d_digits = nullptr;
+    // the residues rebuilt on the device from d_digits: res64, flags (bit 0 zero), words (optional)
+    uint64_t* d_res64 = nullptr;
+    int32_t* d_rflags = nullptr;
+    uint64_t* d_words = nullptr;
+    uint64_t* d_word_off = nullptr;
+    uint64_t pmax = 0;
+    size_t total_words = 0;
 };
 
 void set_trivial(llg_result* r, uint64_t p) {
@@ -292,9 +302,9 @@ namespace {
 
 void release_group(Group& g) {
     if (g.st) {
-        if (g.d_jobs) cudaFreeAsync(g.d_jobs, g.st);
-        if (g.d_results) cudaFreeAsync(g.d_results, g.st);
-        if (g.d_digits) cudaFreeAsync(g.d_digits, g.st);
+        for (void* ptr : {g.d_jobs, g.d_results, g.d_digits, (void*)g.d_res64, (void*)g.d_rflags, (void*)g.d_words,
+                          (void*)g.d_word_off})
+            if (ptr) cudaFreeAsync(ptr, g.st);
         cudaStreamSynchronize(g.st);
         cudaStreamDestroy(g.st);
     }
@@ -312,7 +322,7 @@ void destroy_batch(llg_batch* b) {
 }
 
 // Allocates and uploads one group's job list (synchronously on the group's stream).
-int setup_group(Group& g) {
+int setup_group(Group& g, bool keep_words) {
     CK(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
     const size_t cnt = g.items.size();
@@ -326,6 +336,21 @@ int setup_group(Group& g) {
     } else {
         CK(cudaMallocAsync(&g.d_results, cnt * sizeof(SmallResult), g.st));
         CK(cudaMallocAsync(&g.d_digits, cnt * (size_t)g.n * sizeof(int64_t), g.st));
+        CK(cudaMallocAsync(&g.d_res64, cnt * sizeof(uint64_t), g.st));
+        CK(cudaMallocAsync(&g.d_rflags, cnt * sizeof(int32_t), g.st));
+        g.pmax = 0;
+        for (const Item& it : g.items) g.pmax = std::max(g.pmax, it.p);
+        if (keep_words) {
+            std::vector<uint64_t> off(cnt);
+            g.total_words = 0;
+            for (size_t i = 0; i < cnt; ++i) {
+                off[i] = g.total_words;
+                g.total_words += (size_t)((g.items[i].p + 63) / 64);
+            }
+            CK(cudaMallocAsync(&g.d_words, g.total_words * sizeof(uint64_t), g.st));
+            CK(cudaMallocAsync(&g.d_word_off, cnt * sizeof(uint64_t), g.st));
+            CK(cudaMemcpyAsync(g.d_word_off, off.data(), cnt * sizeof(uint64_t), cudaMemcpyHostToDevice, g.st));
+        }
     }
     CK(cudaMemcpyAsync(g.d_jobs, jobs.data(), cnt * sizeof(SmallJob), cudaMemcpyHostToDevice, g.st));
     CK(cudaStreamSynchronize(g.st));
@@ -350,7 +375,7 @@ int launch_group(llg_batch* b, Group& g, cudaStream_t caller) {
         if (rc) return rc;
         float* elog = (cnt == 1) ? b->d_errlog : nullptr;
         CK(launch_small_fp64(ilog2_exact(g.n), (const SmallJob*)g.d_jobs, cnt, qtw, (int64_t*)g.d_digits,
-                             (SmallResult*)g.d_results, elog, kAbortErr, g.st));
+                             (SmallResult*)g.d_results, elog, g_abort_err.load(), g.st));
     } else {
         int r0 = 0, ll = 0;
         mixed_length_supported(g.n, &r0, &ll);
@@ -360,7 +385,12 @@ int launch_group(llg_batch* b, Group& g, cudaStream_t caller) {
         if (rc) return rc;
         float* elog = (cnt == 1) ? b->d_errlog : nullptr;
         CK(launch_small_fp64_mixed(g.n, (const SmallJob*)g.d_jobs, cnt, qtwL, qtwM, (int64_t*)g.d_digits,
-                                   (SmallResult*)g.d_results, elog, kAbortErr, g.st));
+                                   (SmallResult*)g.d_results, elog, g_abort_err.load(), g.st));
+    }
+    if (g.n) {
+        // exact residues on the device: only res64 and the zero flag (and words when kept) come back
+        CK(rebuild_batch((const int64_t*)g.d_digits, (const SmallJob*)g.d_jobs, cnt, g.n, g.pmax, g.d_res64,
+                         g.d_rflags, g.d_words, g.d_word_off, g.st));
     }
     CK(cudaEventRecord(g.done, g.st));
     CK(cudaStreamWaitEvent(caller, g.done, 0));
@@ -390,13 +420,23 @@ int collect_group(llg_batch* b, Group& g, std::vector<Item>& retry) {
     }
     const uint32_t n = g.n;
     std::vector<SmallResult> res(cnt);
-    std::vector<int64_t> digits(cnt * (size_t)n);
+    std::vector<uint64_t> r64(cnt), words;
+    std::vector<int32_t> rfl(cnt);
     CK(cudaMemcpyAsync(res.data(), g.d_results, cnt * sizeof(SmallResult), cudaMemcpyDeviceToHost, g.st));
-    CK(cudaMemcpyAsync(digits.data(), g.d_digits, digits.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, g.st));
+    CK(cudaMemcpyAsync(r64.data(), g.d_res64, cnt * sizeof(uint64_t), cudaMemcpyDeviceToHost, g.st));
+    CK(cudaMemcpyAsync(rfl.data(), g.d_rflags, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost, g.st));
+    if (b->keep_words) {
+        words.resize(g.total_words);
+        CK(cudaMemcpyAsync(words.data(), g.d_words, g.total_words * sizeof(uint64_t), cudaMemcpyDeviceToHost, g.st));
+    }
     CK(cudaStreamSynchronize(g.st));
+    size_t woff = 0;
     for (size_t i = 0; i < cnt; ++i) {
         const Item& it = g.items[i];
         llg_result& r = b->out[it.idx];
+        const size_t nw = (size_t)((it.p + 63) / 64);
+        const size_t my_off = woff;
+        woff += nw;
         r.max_err = std::max(r.max_err, res[i].max_err);
         r.seconds += (double)res[i].ns * 1e-9;
         if (res[i].status == LLG_ST_ROUNDOFF) {
@@ -416,25 +456,17 @@ int collect_group(llg_batch* b, Group& g, std::vector<Item>& retry) {
         r.iters = res[i].iters_done;
         r.n = n;
         r.escalations = it.escalations;
-        int32_t z = 0;
-        uint64_t* w = nullptr;
-        const size_t nw = (size_t)((it.p + 63) / 64);
-        if (b->keep_words) {
-            b->words[it.idx].assign(nw, 0);
-            w = b->words[it.idx].data();
-        }
-        const int rc = llg_residue_from_digits(it.p, n, digits.data() + i * (size_t)n, w, nw, &r.res64, &z);
-        if (rc) return rc;
-        r.is_zero = z;
+        if (rfl[i] & 2) return fail(LLG_E_CUDA, "device residue rebuild did not settle (p=%llu)", (unsigned long long)it.p);
+        if (b->keep_words) b->words[it.idx].assign(words.begin() + my_off, words.begin() + my_off + nw);
+        r.res64 = r64[i];
+        r.is_zero = (rfl[i] & 1) ? 1 : 0;
         r.status = LLG_OK;
     }
     return LLG_OK;
 }
 
-// One exponent on the two-pass engine: chunks of squarings with a round-off check after each;
-// above the threshold the test restarts from s_0 at the next usable length.
+// Squarings between round-off checks (and residue snapshots) of the two-pass engines.
 constexpr uint64_t kCheckChunk = 4096;
-constexpr double kAbortErrLarge = 0.4;
 
 double bits_to_double(unsigned long long b) {
     double d;
@@ -522,81 +554,117 @@ int device_residue(uint64_t p, uint32_t n, const int* d_digits, std::vector<uint
     return LLG_OK;
 }
 
+// One exponent on a two-pass engine, in chunks of kCheckChunk squarings with a round-off check
+// after each. FP64: after every chunk that stayed within the bound (and has more to go), the exact
+// residue is rebuilt on the GPU into a device snapshot; a chunk above the bound is redone from the
+// last snapshot at the next usable length (the words re-digitised there on the GPU), so an
+// escalation repeats at most one chunk. r.seconds is the device time of every attempt.
 template <class TestT>
 int run_large_t(const Item& item, llg_result& r, std::vector<uint64_t>* words, cudaStream_t st) {
+    constexpr bool kFp64 = std::is_same<TestT, LargeTest>::value;  // the NTT is exact: no checkpoints
+    const uint64_t p = item.p;
+    const size_t nw = (size_t)((p + 63) / 64);
     uint32_t n = item.n;
     uint32_t esc = item.escalations;
-    cudaEvent_t e0, e1;
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    const double abort_err = g_abort_err.load();
+    uint64_t* snap = nullptr;    // residue after snap_iters squarings (device words)
+    uint64_t snap_iters = 0;     // 0: the snapshot is s_0 = 4 itself
+    double total_ms = 0.0, worst = 0.0;
+    auto cleanup = [&] {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (snap) cudaFreeAsync(snap, st);
+    };
+    auto bail = [&](int rc) {
+        cleanup();
+        return rc;
+    };
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+        return bail(fail(LLG_E_CUDA, "creating events"));
+    if (kFp64 && item.iters > kCheckChunk && cudaMallocAsync(&snap, nw * sizeof(uint64_t), st) != cudaSuccess)
+        return bail(fail(LLG_E_NOMEM, "allocating the residue snapshot"));
     for (;;) {
         TestT T;
-        CK(init_large(T, item.p, ilog2_exact(n)));
-        CK(cudaEventRecord(e0, st));
-        CK(T.start(seed_digits(n), st));
-        uint64_t left = item.iters - 1;
-        bool abort = false;
-        double worst = 0.0;
-        while (left > 0 && !abort) {
-            const uint64_t k = std::min(left, kCheckChunk);
-            CK(T.step(k, st));
-            left -= k;
-            LargeCtl h;
-            CK(T.read_ctl(h, st));
-            if (h.timeout) {
-                cudaEventDestroy(e0);
-                cudaEventDestroy(e1);
-                return fail(LLG_E_TIMEOUT, "carry wait timed out (p=%llu)", (unsigned long long)item.p);
+        cudaError_t ce = init_large(T, p, ilog2_exact(n));
+        if (ce == cudaSuccess) ce = cudaEventRecord(e0, st);
+        if (ce == cudaSuccess) {
+            if (snap_iters == 0) {
+                ce = T.start(seed_digits(n), st);
+            } else {
+                ce = digits_from_words(p, n, snap, T.digits, st);
+                if (ce == cudaSuccess) ce = T.start_device(st);
             }
-            worst = bits_to_double(h.err_max);
-            if (worst > kAbortErrLarge) abort = true;
+        }
+        if (ce != cudaSuccess) return bail(fail(ce == cudaErrorMemoryAllocation ? LLG_E_NOMEM : LLG_E_CUDA, "CUDA: %s", cudaGetErrorString(ce)));
+        uint64_t done = snap_iters + 1;
+        bool abort = false;
+        double err = 0.0;
+        while (done < item.iters && !abort) {
+            const uint64_t k = std::min(item.iters - done, kCheckChunk);
+            LargeCtl h;
+            ce = T.step(k, st);
+            if (ce == cudaSuccess) ce = T.read_ctl(h, st);
+            if (ce != cudaSuccess) return bail(fail(LLG_E_CUDA, "CUDA: %s", cudaGetErrorString(ce)));
+            if (h.timeout) return bail(fail(LLG_E_TIMEOUT, "carry wait timed out (p=%llu)", (unsigned long long)p));
+            done += k;
+            err = bits_to_double(h.err_max);
+            if (err > abort_err) {
+                abort = true;
+            } else if (kFp64 && snap && done < item.iters) {
+                // checkpoint: the exact residue of this clean state, kept on the device
+                ce = T.final_pass(st);
+                if (ce != cudaSuccess) return bail(fail(LLG_E_CUDA, "CUDA: %s", cudaGetErrorString(ce)));
+                int32_t z = 0;
+                uint64_t r64 = 0;
+                const int rc = llg_residue_from_digits_device(p, n, T.digits, snap, &r64, &z, st);
+                if (rc) return bail(fail(rc, "residue snapshot on the device failed"));
+                snap_iters = done;
+            }
         }
         if (!abort) {
-            CK(T.final_pass(st));
-            CK(cudaEventRecord(e1, st));
             LargeCtl h;
-            CK(T.read_ctl(h, st));
-            worst = bits_to_double(h.err_max);
-            if (h.timeout) {
-                cudaEventDestroy(e0);
-                cudaEventDestroy(e1);
-                return fail(LLG_E_TIMEOUT, "carry wait timed out (p=%llu)", (unsigned long long)item.p);
-            }
-            if (worst > kAbortErrLarge) abort = true;
+            ce = T.final_pass(st);
+            if (ce == cudaSuccess) ce = cudaEventRecord(e1, st);
+            if (ce == cudaSuccess) ce = T.read_ctl(h, st);
+            if (ce != cudaSuccess) return bail(fail(LLG_E_CUDA, "CUDA: %s", cudaGetErrorString(ce)));
+            if (h.timeout) return bail(fail(LLG_E_TIMEOUT, "carry wait timed out (p=%llu)", (unsigned long long)p));
+            err = bits_to_double(h.err_max);
+            if (err > abort_err) abort = true;
+        } else if (cudaEventRecord(e1, st) != cudaSuccess) {
+            return bail(fail(LLG_E_CUDA, "recording an event"));
         }
-        r.max_err = std::max(r.max_err, worst);
+        float ms = 0.f;
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+            return bail(fail(LLG_E_CUDA, "timing the attempt"));
+        total_ms += ms;
+        worst = std::max(worst, err);
         if (abort) {  // FP64 only: the NTT's round-off is identically zero
-            const uint32_t nn = next_fp64_length(item.p, n);
+            const uint32_t nn = next_fp64_length(p, n);
             if (!nn) {
                 r.status = LLG_E_ROUNDOFF;
                 r.n = n;
                 r.escalations = esc;
+                r.max_err = worst;
                 break;
             }
             n = nn;
             ++esc;
             continue;
         }
-        float ms = 0;
-        CK(cudaEventElapsedTime(&ms, e0, e1));
         int32_t z = 0;
-        const int rc = device_residue(item.p, n, T.digits, words, nullptr, 0, &r.res64, &z, st);
-        if (rc) {
-            cudaEventDestroy(e0);
-            cudaEventDestroy(e1);
-            return rc;
-        }
+        const int rc = device_residue(p, n, T.digits, words, nullptr, 0, &r.res64, &z, st);
+        if (rc) return bail(rc);
         r.iters = item.iters;
         r.is_zero = z;
         r.n = n;
         r.escalations = esc;
-        r.seconds = ms * 1e-3;
-        r.max_err = worst;
+        r.seconds = total_ms * 1e-3;
+        r.max_err = err;  // the round-off of the attempt that produced the result
         r.status = LLG_OK;
         break;
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    cleanup();
     return LLG_OK;
 }
 
@@ -663,7 +731,7 @@ int make_batch(const uint64_t* ps, size_t count, uint64_t max_iters, int engine,
     // largest lengths first (they run longest)
     std::sort(b->groups.begin(), b->groups.end(), [](const Group& x, const Group& y) { return x.n > y.n; });
     for (Group& g : b->groups) {
-        if ((rc = setup_group(g))) {
+        if ((rc = setup_group(g, b->keep_words))) {
             destroy_batch(b);
             return rc;
         }
@@ -722,7 +790,7 @@ int collect_batch(llg_batch* b) {
             Group g;
             g.n = kv.first;
             g.items = std::move(kv.second);
-            int rc = setup_group(g);
+            int rc = setup_group(g, b->keep_words);
             if (!rc) {
                 CK(cudaEventRecord(b->fork, g.st));
                 rc = launch_group(b, g, g.st);
@@ -835,6 +903,14 @@ int llg_get_large_split(int log_n, int* rows) {
     if (rows) *rows = v >= 0 ? shape_rows(v) : large_rows_per_block(lc);
     return lc;
 }
+
+int llg_set_roundoff_limit(double limit) {
+    if (!(limit > 0.0 && limit < 0.5)) return fail(LLG_E_ARG, "round-off limit %g outside (0, 0.5)", limit);
+    g_abort_err.store(limit);
+    return LLG_OK;
+}
+
+double llg_get_roundoff_limit(void) { return g_abort_err.load(); }
 
 int llg_set_max_bpw(double b) {
     if (!(b >= 2.0 && b <= (double)kMaxDigitBits)) return fail(LLG_E_ARG, "bits per word %g out of range [2, 28]", b);
@@ -1025,7 +1101,7 @@ int llg_test_read(llg_test* t, void* stream, llg_result* out, uint64_t* words, s
     const int rc = device_residue(p, out->n, dd, nullptr, words, words ? nwords : 0, &out->res64, &z, st);
     if (rc) return rc;
     out->is_zero = z;
-    out->status = out->max_err > kAbortErrLarge ? LLG_E_ROUNDOFF : LLG_OK;
+    out->status = out->max_err > g_abort_err.load() ? LLG_E_ROUNDOFF : LLG_OK;
     return LLG_OK;
 }
 
@@ -1034,6 +1110,36 @@ int llg_test_time_passes(llg_test* t, uint64_t iters, void* stream, double* row_
     cudaStream_t st = stream ? (cudaStream_t)stream : default_stream_for_thread();
     if (t->f) CK(t->f->time_passes(iters, st, *row_us, *col_us));
     else CK(t->n->time_passes(iters, st, *row_us, *col_us));
+    return LLG_OK;
+}
+
+int llg_test_load(llg_test* t, const uint64_t* words, size_t nwords, uint64_t iters_done, void* stream) {
+    if (!t || !words) return fail(LLG_E_ARG, "null pointer");
+    const uint64_t p = t->p();
+    const size_t nw = (size_t)((p + 63) / 64);
+    if (nwords < nw) return fail(LLG_E_ARG, "words buffer too small (%zu < %zu)", nwords, nw);
+    if (p % 64 && (words[nw - 1] >> (p % 64)) != 0) return fail(LLG_E_ARG, "residue has bits at or above p");
+    cudaStream_t st = stream ? (cudaStream_t)stream : default_stream_for_thread();
+    uint64_t* dw = nullptr;
+    CK(cudaMallocAsync(&dw, nw * sizeof(uint64_t), st));
+    cudaError_t e = cudaMemcpyAsync(dw, words, nw * sizeof(uint64_t), cudaMemcpyHostToDevice, st);
+    int* digits = t->f ? t->f->digits : t->n->digits;
+    if (e == cudaSuccess) e = digits_from_words(p, 1ull << t->logN(), dw, digits, st);
+    if (e == cudaSuccess) e = t->f ? t->f->start_device(st) : t->n->start_device(st);
+    cudaFreeAsync(dw, st);
+    if (e != cudaSuccess) return fail(LLG_E_CUDA, "CUDA: %s", cudaGetErrorString(e));
+    if (t->f) t->f->done = iters_done + 1;
+    else t->n->done = iters_done + 1;
+    return LLG_OK;
+}
+
+int llg_test_diag_withhold_wrap(llg_test* t, uint64_t spin_limit, void* stream) {
+    if (!t) return fail(LLG_E_ARG, "null test");
+    if (!t->f) return fail(LLG_E_ARG, "the withheld-wrap diagnostic is for the FP64 engine");
+    cudaStream_t st = stream ? (cudaStream_t)stream : default_stream_for_thread();
+    bool timed_out = false;
+    CK(t->f->diag_withhold_wrap(spin_limit, st, timed_out));
+    if (timed_out) return fail(LLG_E_TIMEOUT, "carry wait timed out (wrap-around job withheld)");
     return LLG_OK;
 }
 

@@ -38,6 +38,9 @@ struct SmallGeom {
 };
 
 __device__ __forceinline__ int phys(int x) { return x + (x >> 4); }
+// Exchange-buffer padding of one slot per 2^PADLOG (phys is PADLOG = 4).
+template <int PADLOG>
+__device__ __forceinline__ int physp(int x) { return x + (x >> PADLOG); }
 
 // Frequency index k of DIF output position pos (mixed radix E,...,E,RLAST digit reversal).
 template <class G>
@@ -104,7 +107,10 @@ __device__ __forceinline__ double2 twiddle_g(const double2* __restrict__ q, uint
 // Forward (INV=false) or inverse radix pass S on the register array v (E values).
 // Forward: load (S > 0), DFT, twiddle w_L^{n2 k1}, store (S < P-1).
 // Inverse: load (S < P-1), conj twiddle, inverse DFT, store (S > 0).
-template <class G, int S, bool INV, bool SYNC_BEFORE_STORE, class SYNC>
+// ES: element stride of the exchange buffer. Slot x of this transform is buf[physp<PADLOG>(x) * ES],
+// so ES transforms can share one buffer interleaved (transform r at buf + r), as the row pass of
+// the two-pass engine does with the rows of a tile.
+template <class G, int S, bool INV, bool SYNC_BEFORE_STORE, class SYNC, int ES = 1, int PADLOG = 4>
 __device__ __forceinline__ void radix_pass(double2 (&v)[G::E], double2* __restrict__ buf,
                                            const double2* __restrict__ qtw, int t, const SYNC& sync) {
     constexpr int R = G::radix(S);
@@ -113,23 +119,25 @@ __device__ __forceinline__ void radix_pass(double2 (&v)[G::E], double2* __restri
     constexpr int B = G::E / R;
     constexpr bool LOAD = INV ? (S < G::P - 1) : (S > 0);
     constexpr bool STORE = INV ? (S > 0) : (S < G::P - 1);
-    // phys(base + n1 ST) = phys(base) + n1 * DST whenever the R slots of a butterfly never cross a
-    // 16-slot boundary out of step with base: ST a multiple of 16, or the whole group (L slots,
-    // 16-aligned) inside one 16-slot block. The offsets are then compile-time constants.
-    constexpr bool AFFINE = (ST % 16 == 0) || (L <= 16);
-    constexpr int DST = (ST % 16 == 0) ? ST + ST / 16 : ST;
+    // physp(base + n1 ST) = physp(base) + n1 * DST whenever the R slots of a butterfly never cross a
+    // padding boundary (every 2^PADLOG slots) out of step with base: ST a multiple of 2^PADLOG, or
+    // the whole group (L slots, L-aligned) inside one padding block. The offsets are then
+    // compile-time constants.
+    constexpr int PB = 1 << PADLOG;
+    constexpr bool AFFINE = (ST % PB == 0) || (L <= PB);
+    constexpr int DST = (ST % PB == 0) ? ST + ST / PB : ST;
 #pragma unroll
     for (int h = 0; h < B; ++h) {
         const int beta = t * B + h;
         const int g = beta / ST, n2 = beta % ST;
         const int base = g * L + n2;
-        const int pbase = phys(base);
+        const int pbase = physp<PADLOG>(base);
         double2* vv = v + h * R;
         if constexpr (LOAD) {
 #pragma unroll
             for (int n1 = 0; n1 < R; ++n1) {
-                const int x = AFFINE ? pbase + n1 * DST : phys(base + n1 * ST);
-                vv[n1] = buf[x];
+                const int x = AFFINE ? pbase + n1 * DST : physp<PADLOG>(base + n1 * ST);
+                vv[n1] = buf[x * ES];
             }
         }
         if constexpr (!INV) {
@@ -150,8 +158,8 @@ __device__ __forceinline__ void radix_pass(double2 (&v)[G::E], double2* __restri
         if constexpr (STORE && !SYNC_BEFORE_STORE) {
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1) {
-                const int x = AFFINE ? pbase + k1 * DST : phys(base + k1 * ST);
-                buf[x] = vv[k1];
+                const int x = AFFINE ? pbase + k1 * DST : physp<PADLOG>(base + k1 * ST);
+                buf[x * ES] = vv[k1];
             }
         }
     }
@@ -162,37 +170,37 @@ __device__ __forceinline__ void radix_pass(double2 (&v)[G::E], double2* __restri
             const int beta = t * B + h;
             const int g = beta / ST, n2 = beta % ST;
             const int base = g * L + n2;
-            const int pbase = phys(base);
+            const int pbase = physp<PADLOG>(base);
 #pragma unroll
             for (int k1 = 0; k1 < R; ++k1) {
-                const int x = AFFINE ? pbase + k1 * DST : phys(base + k1 * ST);
-                buf[x] = v[h * R + k1];
+                const int x = AFFINE ? pbase + k1 * DST : physp<PADLOG>(base + k1 * ST);
+                buf[x * ES] = v[h * R + k1];
             }
         }
     }
 }
 
 // Forward passes S .. P-1 (pass S loads from buf unless S == 0).
-template <class G, int S, class SYNC = CtaSync>
+template <class G, int S, class SYNC = CtaSync, int ES = 1, int PADLOG = 4>
 __device__ __forceinline__ void forward_from(double2 (&v)[G::E], double2* buf, const double2* qtw,
                                              int t, const SYNC& sync = SYNC()) {
     if constexpr (S < G::P) {
-        radix_pass<G, S, false, false>(v, buf, qtw, t, sync);
+        radix_pass<G, S, false, false, SYNC, ES, PADLOG>(v, buf, qtw, t, sync);
         if constexpr (S < G::P - 1) sync();
-        forward_from<G, S + 1, SYNC>(v, buf, qtw, t, sync);
+        forward_from<G, S + 1, SYNC, ES, PADLOG>(v, buf, qtw, t, sync);
     }
 }
 
 // Inverse passes S down to 0, starting from registers. FIRST_SYNC: a barrier between the first
 // pass's arithmetic and its stores (needed when other threads may still read the positions it
 // overwrites, e.g. a partner read of the same buffer).
-template <class G, int S, bool FIRST_SYNC = true, class SYNC = CtaSync>
+template <class G, int S, bool FIRST_SYNC = true, class SYNC = CtaSync, int ES = 1, int PADLOG = 4>
 __device__ __forceinline__ void inverse_from(double2 (&v)[G::E], double2* buf, const double2* qtw,
                                              int t, const SYNC& sync = SYNC()) {
     if constexpr (S >= 0) {
-        radix_pass<G, S, true, FIRST_SYNC && S == G::P - 1>(v, buf, qtw, t, sync);
+        radix_pass<G, S, true, FIRST_SYNC && S == G::P - 1, SYNC, ES, PADLOG>(v, buf, qtw, t, sync);
         if constexpr (S > 0) sync();
-        inverse_from<G, S - 1, false, SYNC>(v, buf, qtw, t, sync);
+        inverse_from<G, S - 1, false, SYNC, ES, PADLOG>(v, buf, qtw, t, sync);
     }
 }
 

@@ -31,7 +31,6 @@ struct LargeTest {
     double2* V = nullptr;
     double* carry = nullptr;
     float* carry2 = nullptr;
-    double* halo = nullptr;
     LargeCtl* ctl = nullptr;
     unsigned* flags = nullptr;
     int* digits = nullptr;
@@ -49,6 +48,7 @@ struct LargeTest {
     // log_c < 0: the default split; rows == 0: the default rows per row-pass block
     cudaError_t init(uint64_t p, int log_n, int log_c = -1, int rows = 0);
     cudaError_t start(const std::vector<int>& digits, cudaStream_t st);  // INIT + first squaring
+    cudaError_t start_device(cudaStream_t st);  // the same from the digits already in `digits`
     cudaError_t step(uint64_t k, cudaStream_t st);                        // k more squarings
     cudaError_t step_plain(uint64_t k, bool dump_last, cudaStream_t st);
     cudaError_t final_pass(cudaStream_t st);                              // FINAL: digits on device
@@ -57,6 +57,10 @@ struct LargeTest {
     cudaError_t clear_err_since(cudaStream_t st);
     // k squarings, one launch at a time with events between the passes: mean device us per pass
     cudaError_t time_passes(uint64_t k, cudaStream_t st, double& row_us, double& col_us);
+    // Diagnostic: one row pass with the wrap-around job withheld and waits bounded by spin_limit
+    // sleeps, so tile 0 and the last tile give up; timed_out reports ctl->timeout. The state is
+    // invalid afterwards.
+    cudaError_t diag_withhold_wrap(unsigned long long spin_limit, cudaStream_t st, bool& timed_out);
 };
 
 // Device state of one exponent on the two-pass NTT engine (same launch sequence as LargeTest).
@@ -74,6 +78,7 @@ struct NttLargeTest {
     ~NttLargeTest();
     cudaError_t init(uint64_t p, int log_n);
     cudaError_t start(const std::vector<int>& digits, cudaStream_t st);
+    cudaError_t start_device(cudaStream_t st);
     cudaError_t step(uint64_t k, cudaStream_t st);
     cudaError_t final_pass(cudaStream_t st);
     cudaError_t finish(cudaStream_t st, std::vector<int>& out);

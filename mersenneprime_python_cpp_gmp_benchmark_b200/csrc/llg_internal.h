@@ -73,21 +73,37 @@ struct NttConst {
 cudaError_t launch_small_ntt(int log_n, const SmallJob* jobs, int njobs, const uint64_t* qtw, NttConst K,
                              int64_t* digits, SmallResult* results, cudaStream_t st);
 
+// Digits (int32, natural order, within one of balanced) at length n of the residue s in d_words
+// (ceil(p/64) little-endian limbs, s < 2^p), formed on the GPU; enqueued on st. n <= p, digits of
+// at most 30 bits.
+cudaError_t digits_from_words(uint64_t p, uint64_t n, const uint64_t* d_words, int32_t* d_digits, cudaStream_t st);
+
+// Exact residues of a whole-test batch on the GPU: cnt exponents (d_jobs[i].p <= pmax), n int64
+// digits each (d_digits, natural order). Per exponent: d_res64[i], d_flags[i] (bit 0: residue zero,
+// bit 1: failure) and, when d_words is non-null, the ceil(p/64) words at d_word_off[i]. Enqueued
+// on st.
+cudaError_t rebuild_batch(const int64_t* d_digits, const SmallJob* d_jobs, int cnt, uint32_t n, uint64_t pmax,
+                          uint64_t* d_res64, int32_t* d_flags, uint64_t* d_words, const uint64_t* d_word_off,
+                          cudaStream_t st);
+
 // ---- two-pass engine (N = 2^16 .. 2^23): state resident in HBM ------------------------------
 
-constexpr int kRowG = 4;              // rows per row-pass block (rows of up to 1024 complex)
-// rows per row-pass block for a row length of 2^log_c complex values (64 KiB of state per block)
+// Row-pass tiles of g rows of 2^log_c complex values that have kernels (LLG_ROW_SHAPES lists
+// them as X(log_c, g)): g * 2^log_c / (values per thread) threads, a multiple of 32 up to 512,
+// and at most ~180 KB of shared memory. large_rows_per_block is the default g of a row length.
+#define LLG_ROW_SHAPES(X) \
+    X(6, 4) X(6, 8) X(7, 2) X(7, 4) X(7, 8) X(8, 2) X(8, 4) X(8, 8) X(9, 2) X(9, 4) X(9, 8) X(10, 2) \
+    X(10, 4) X(10, 8) X(11, 2) X(11, 4)
+constexpr bool large_rows_supported(int log_c, int g) {
+    return (log_c >= 6 && log_c <= 11) && (g == 2 || g == 4 || g == 8) && !(log_c == 6 && g == 2) &&
+           !(log_c == 11 && g == 8);
+}
 #ifdef __CUDACC__
 __host__ __device__
 #endif
-constexpr int large_rows_per_block(int log_c) { return log_c >= 11 ? 2 : kRowG; }
-// row-pass shapes with kernels: 4 rows per block for rows of 2^6 .. 2^11, 2 rows for 2^8 .. 2^11,
-// 8 rows for 2^9 .. 2^10 (the larger the block, the longer the contiguous runs of its loads)
-constexpr bool large_rows_supported(int log_c, int g) {
-    return (g == 4 && log_c >= 6 && log_c <= 11) || (g == 2 && log_c >= 8 && log_c <= 11) ||
-           (g == 8 && log_c >= 9 && log_c <= 10);
-}
-constexpr int kLargeLogE = 4;         // log2 of the complex values per thread in the two-pass kernels
+constexpr int large_rows_per_block(int log_c) { return log_c >= 11 ? 2 : 4; }
+constexpr int kLargeLogE = 4;         // log2 of the complex values per thread in the column pass
+constexpr unsigned long long kSpinLimit = 1ull << 22;  // x ~64 ns sleeps: ~0.3 s, then give up + flag
 // log2 of the complex values per thread in the row pass of g rows of 2^log_c complex: 8 values
 // (radix-8 passes, 64 registers a thread, two or more blocks per SM) for rows of up to 2^9, 16
 // (radix-16 passes, 128 registers) for longer rows
@@ -102,7 +118,7 @@ struct LargeCtl {
     unsigned int timeout;            // set when a bounded wait gave up (the result is then invalid)
     unsigned long long err_max;      // bits of the max round-off over the run (double, >= 0)
     unsigned long long err_since;    // same, since the host last cleared it
-    unsigned int halo_read;          // epoch + 1 once block 0 has read the wrap-around rows
+    unsigned int halo_read;          // NTT: epoch + 1 once block 0 has read the wrap-around rows
 };
 
 enum { LARGE_INIT = 0, LARGE_ITER = 1, LARGE_FINAL = 2 };
@@ -138,11 +154,12 @@ struct LargeArgs {
     const double* wB;         // [C] 2^(sB/N)
     const double* iwB;        // [C] 2^(-sB/N) / (4M)
     const int* sB;            // [C] (-2Rb p) mod N
-    double* carry;            // [nblocks][C] hop-1 carry-outs of each block's last row (integers)
-    float* carry2;            // [nblocks][C] hop-2 carry-outs (integers of a few units)
-    double* halo;             // [2][C] block 0's wrap-around carries (hop 2, hop 3)
+    double* carry;            // [nblocks + 1][C] hop-1 carry-outs of a tile's last row (integers):
+                              // slot 0 the wrap-around job's (row R-1, one column on), k + 1 tile k's
+    float* carry2;            // [nblocks + 1][C] hop-2 carry-outs (integers of a few units)
     LargeCtl* ctl;
-    unsigned int* flags;      // [nblocks] epoch + 1 once block k published its carries
+    unsigned int* flags;      // [nblocks + 1] epoch + 1 once the job of that slot published its carries
+    unsigned long long spin_limit;  // bound of every wait on a flag (x ~64 ns sleeps)
     int* digits;              // N int32, natural order (INIT input; dump / FINAL output)
     float* errlog;            // per-epoch max round-off ring (may be null)
     int errlog_len;
@@ -153,7 +170,8 @@ struct LargeArgs {
     int logN;
 };
 
-cudaError_t launch_large_row(int log_c, int g, int mode, const LargeArgs& a, cudaStream_t st);
+// Row pass; grid > 0 overrides the block count (nblocks, + 1 for the wrap-around job unless INIT).
+cudaError_t launch_large_row(int log_c, int g, int mode, const LargeArgs& a, cudaStream_t st, int grid = 0);
 cudaError_t launch_large_col(int log_r, const LargeArgs& a, cudaStream_t st);
 
 // ---- two-pass exact NTT engine (N = 2^14 .. 2^23): N field elements in HBM ------------------

@@ -7,7 +7,7 @@
 // lucaslehmer.cpp:283,288, and an O(N) host loop for each of weight, unweight and carry,
 // lucaslehmer.cpp:282,289-310):
 //
-//   row pass (one block = G consecutive rows, G = 2, 4 or 8, all C columns):
+//   row pass (one block = a tile of G consecutive rows, G = 2, 4 or 8, all C columns):
 //       inverse C-point FFT                                   (end of the previous squaring)
 //       unweight, round, max round-off, carry, "- 2"
 //       weight, forward C-point FFT                           (start of this squaring)
@@ -15,22 +15,29 @@
 //       twiddle w_M^{ac}, forward R-point FFT, real-FFT split + pointwise square over the pair
 //       (k, M-k), inverse R-point FFT, twiddle w_M^{-ac}
 //
-// The state is stored column-slot-major (element (a, pos) at pos*R + a), so a row block reads
-// and writes G contiguous complex values (16 G bytes) per column slot and a column block reads
-// and writes its columns contiguously.
+// The state is stored column-slot-major (element (a, pos) at pos*R + a), so a row tile reads and
+// writes G contiguous complex values (16 G bytes) per column slot and a column block reads and
+// writes its columns contiguously.
+//
+// Row tiles interleave their rows across the lanes of every warp: thread t works on row t % G of
+// the tile at FFT thread index t / G. A tile's loads and stores then go straight between HBM and
+// registers in runs of 16 G bytes (no shared-memory transpose), the FFT exchange buffer holds
+// slot x of row r at physp(x) * G + r (a quarter warp touches one contiguous 16 G-byte run:
+// conflict-free), and the carry between the rows of a tile is a shuffle between neighbouring
+// lanes.
 //
 // Carry. Digits 2m, 2m+1 of row a carry into row a+1 (m -> m+1 is a -> a+1), so the chain runs
 // down the rows of each column b. Each row's carry-out is computed from that row's rounded values
-// alone (two-digit chain started at zero); the incoming carry is folded into the first digit and
-// the small remainder into the second, which keeps every digit within a few units of balanced and
-// makes carry-outs independent of carry-ins. Inside a block the carries pass through shared
-// memory; between blocks block k publishes its last row's carry-outs and a flag, and block k+1
-// reads them after a bounded wait. Only the block's first row waits for that flag (and its
-// second row for the first row's result): the other rows finish their carries from inside the
-// block and go on to the forward FFT meanwhile. Blocks take tickets in launch order, so the block waited on is
-// always resident or finished. The wrap-around carry into row 0 (2^p == 1) comes from row R-1;
-// block 0 runs the last block's rows through the same code first, instead of waiting on the last
-// block, and the last block waits (bounded) until block 0 has read them before overwriting them.
+// alone (two-digit chain started at zero: hop 1); the incoming carry is folded into the first
+// digit and split again (hop 2), and the small remainder of that split goes into the next row's
+// first digit (hop 3). That keeps every digit within a few units of balanced and makes carry-outs
+// independent of carry-ins. Inside a tile the carries pass between lanes; between tiles, tile k
+// publishes its last row's hop-1 and hop-2 carry-outs and a flag, and tile k+1 reads them after a
+// bounded wait. Tiles take tickets in launch order, so the tile waited on is always resident or
+// finished. The wrap-around carry into row 0 (2^p == 1) comes from row R-1: the first ticket is a
+// separate job that runs the last tile's rows through the inverse FFT and hops 1-2 and publishes
+// their carry-outs (one column on) in the slot tile 0 reads; the last tile waits (bounded) for
+// that job before overwriting those rows.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -44,8 +51,6 @@
 namespace llg {
 
 namespace {
-
-constexpr unsigned long long kSpinLimit = 1ull << 22;  // x ~64 ns: ~0.3 s, then give up + flag
 
 __device__ __forceinline__ double2 twiddle_M(const LargeArgs& A, uint32_t x, bool inv) {
     const double2 a = __ldg(A.tw1 + (x & ((1u << A.tw_shift) - 1u)));
@@ -61,281 +66,191 @@ __host__ __device__ constexpr int large_row_threads(int log_c, int g) {
 }
 // blocks per SM the row kernel is built for: 128 registers a thread at 16 values, 64 at 8
 __host__ __device__ constexpr int large_row_min_blocks(int log_c, int g) {
-    const int t = large_row_threads(log_c, g) < 32 ? 32 : large_row_threads(log_c, g);
-    const int b = (large_row_log_e(log_c, g) >= 4 ? 512 : 1024) / t;
-    return b > 16 ? 16 : b;
+    const int b = (large_row_log_e(log_c, g) >= 4 ? 512 : 1024) / large_row_threads(log_c, g);
+    return b > 16 ? 16 : (b < 1 ? 1 : b);
+}
+// exchange-buffer slots of a tile: G rows of C + C/E padded slots
+__host__ __device__ constexpr int large_row_slots(int log_c, int g) {
+    return g * ((1 << log_c) + ((1 << log_c) >> large_row_log_e(log_c, g)));
 }
 
 template <int LOG_C, int G, int MODE>
 __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blocks(LOG_C, G))
     large_row(const LargeArgs A) {
-    using GC = SmallG<LOG_C, large_row_log_e(LOG_C, G), TW_FULL>;  // full twiddle table
+    constexpr int LE = large_row_log_e(LOG_C, G);
+    using GC = SmallG<LOG_C, LE, TW_FULL>;  // full twiddle table
     constexpr int C = GC::M, TR = GC::T, E = GC::E, T = G * TR;
-    static_assert(T % 32 == 0, "whole warps");
+    static_assert(T % 32 == 0 && 32 % G == 0, "whole warps of whole row groups");
+    constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int RS = GC::PAD + 1;  // row-buffer stride: odd, so the rows of a slot hit different banks
     constexpr int QL = (int)twiddle_table_len<GC>();
-    double2* bufs = reinterpret_cast<double2*>(smem_raw);  // G exchange buffers of RS slots
-    double2* qtw = bufs + G * RS;                            // padded twiddle table (C-point)
-    double* carr = reinterpret_cast<double*>(bufs);          // G x C hop-1 carry-outs (reuses bufs)
-    double* carr2 = carr + G * C;                            // G x C hop-2 carry-outs
-    double* late = reinterpret_cast<double*>(qtw + QL);     // C: row 0's hop-2 carry-outs, for row 1
-    double* hin = reinterpret_cast<double*>(A.halo);         // C: wrap carry into row 0 (hop 2)
-    double* hin2 = hin + C;                                  // C: wrap carry into row 0 (hop 3)
+    double2* xbuf = reinterpret_cast<double2*>(smem_raw);          // exchange: slot physp(x) * G + row
+    double2* qtw = xbuf + large_row_slots(LOG_C, G);               // padded twiddle table (C-point)
     __shared__ unsigned long long s_err;
-    __shared__ int s_blk;
+    __shared__ int s_job;
     __shared__ unsigned s_epoch;
 
-    const int t = threadIdx.x, rg = t / TR, tr = t % TR;
-    double2* buf = bufs + rg * RS;
+    const int t = threadIdx.x, ra = t % G, tr = t / G;
+    double2* buf = xbuf + ra;
     const int N = 1 << A.logN, R = A.R;
-    // each row's FFT exchanges wait only on that row's warps (named barrier 1 + rg)
-    using RowSync = typename std::conditional<(TR >= 32), NamedSync, CtaSync>::type;
-    RowSync gsync;
-    if constexpr (TR >= 32) gsync = NamedSync{1u + (unsigned)rg, (unsigned)TR};
+    const CtaSync sync;
 
     if (t == 0) {
         const unsigned ep = *reinterpret_cast<volatile unsigned*>(&A.ctl->epoch);
         s_epoch = ep;
         if (MODE == LARGE_INIT) {
-            s_blk = blockIdx.x;
+            s_job = blockIdx.x;
         } else {
-            const int b = (int)atomicAdd(&A.ctl->ticket[ep & 1], 1u);
-            if (b == A.nblocks - 1) {
+            // tickets in launch order: ticket 0 is the wrap-around job, ticket k tile k - 1
+            const int tk = (int)atomicAdd(&A.ctl->ticket[ep & 1], 1u);
+            if (tk == A.nblocks) {
                 // every block of this launch holds its ticket: both counters can be reset
                 A.ctl->ticket[(ep + 1) & 1] = 0u;
                 A.ctl->ticket[ep & 1] = 0u;
             }
-            s_blk = b;
+            s_job = tk - 1;
         }
         s_err = 0ull;
     }
     __syncthreads();
-    const int blk = s_blk;
+    const int job = s_job;  // -1: the wrap-around job (rows R-G .. R-1), else the tile
     const unsigned ep = s_epoch;
-    const int a0 = blk * G;
-    const int a = a0 + rg;
-    // digit sizes: b = q or q + 1 bits, as 2^b and 2^-b
-    const double pw0 = pow2(A.q), pw1 = pow2(A.q + 1), iv0 = pow2(-A.q), iv1 = pow2(-A.q - 1);
-    // column weight exponent sB(b) = (-2 R b p) mod N, from 32-bit products (N <= 2^23 < 2^32)
+    const bool wrap_job = job < 0;
+    const int a = (wrap_job ? R - G : job * G) + ra;  // this thread's row
+    // weight exponent s = (sA(2a+e) + sB(b)) mod N of digit 2m+e; sB(b) = (-2 R b p) mod N from
+    // 32-bit products (N <= 2^23 < 2^32). digit_kind(b) gives bit 0 / 1: digit 0 / 1 of (a, b) has
+    // q + 1 bits (s < p mod N); bit 2 / 3: sA + sB wrapped past N, so the weight 2^(s/N) is the
+    // table product times 1/2 (and the inverse weight times 2). Recomputed where used: a few
+    // integer operations, fewer live registers than keeping them.
+    const int sA0 = __ldg(A.sA + 2 * a), sA1 = __ldg(A.sA + 2 * a + 1);
     const uint32_t kB = (uint32_t)(2 * R) * (uint32_t)A.rem;
-    auto sB_of = [&](int b) { return (int)((0u - kB * (uint32_t)b) & (uint32_t)(N - 1)); };
+    auto digit_kind = [&](int b) {
+        const int sb = (int)((0u - kB * (uint32_t)b) & (uint32_t)(N - 1));
+        const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
+        const int s0 = o0 ? sA0 + sb - N : sA0 + sb, s1 = o1 ? sA1 + sb - N : sA1 + sb;
+        return (uint32_t)(s0 < A.rem) | ((uint32_t)(s1 < A.rem) << 1) | ((uint32_t)o0 << 2) | ((uint32_t)o1 << 3);
+    };
 
     double2 v[E];
-    double x0s[E], x1s[E];
-
     if constexpr (MODE == LARGE_INIT) {
 #pragma unroll
         for (int i = 0; i < E; ++i) {
-            const int b = tr + TR * i;
-            const size_t m = (size_t)a + (size_t)R * b;
+            const size_t m = (size_t)a + (size_t)R * (tr + TR * i);
             const int2 d = *reinterpret_cast<const int2*>(A.digits + 2 * m);
-            x0s[i] = (double)d.x;
-            x1s[i] = (double)d.y;
+            v[i] = make_double2((double)d.x, (double)d.y);
         }
         for (int k = t; k < QL; k += T) qtw[k] = A.qtwC[k];
         __syncthreads();
     } else {
-        double lerr = 0.0;
-        // Phase 0 (block 0 only): the last block's rows R-G .. R-1 through the same inverse FFT
-        // and hops 1-2, for the carry-outs of row R-1 that wrap into row 0 (2^p == 1), exactly as
-        // the last block computes and publishes them. Phase 1: the block's own rows.
-#pragma unroll 1
-        for (int ph = (blk == 0) ? 0 : 1; ph < 2; ++ph) {
-            const int base = ph ? a0 : R - G;
-            const int ar = base + rg;
-            // ---- load rows base .. base+G-1 (coalesced: G contiguous values per column slot) ----
-            {
-                double2 tmp[G * C / T];
+        // ---- the tile's rows, straight into registers: thread (row, tr) holds positions
+        //      tr E .. tr E + E-1 (the forward FFT's output order), G rows per 16 G-byte run ----
 #pragma unroll
-                for (int r = 0; r < G * C / T; ++r) {
-                    const int qq = t + T * r, pos = qq / G, ra = qq % G;
-                    tmp[r] = A.V[(size_t)pos * R + base + ra];
-                }
-                // the twiddle table (L2-resident) is fetched while the rows' loads are in flight
-                if (ph == 0 || blk != 0)
-                    for (int k = t; k < QL; k += T) qtw[k] = A.qtwC[k];
-#pragma unroll
-                for (int r = 0; r < G * C / T; ++r) {
-                    const int qq = t + T * r, pos = qq / G, ra = qq % G;
-                    bufs[ra * RS + phys(pos)] = tmp[r];
-                }
-            }
-            __syncthreads();
-            if (ph == 0 && t == 0) {
-                // rows R-G .. R-1 are read: the last block may overwrite them
-                __threadfence();
-                *reinterpret_cast<volatile unsigned*>(&A.ctl->halo_read) = ep + 1u;
-            }
-#pragma unroll
-            for (int j = 0; j < E; ++j) v[j] = buf[phys(tr * E + j)];
-            inverse_from<GC, GC::P - 1, false>(v, buf, qtw, tr, gsync);
-            __syncthreads();  // the exchange buffers become the carry arrays
+        for (int j = 0; j < E; ++j) v[j] = __ldcg(A.V + (size_t)(tr * E + j) * R + a);
+        // the twiddle table (L2-resident) is fetched while the rows' loads are in flight
+        for (int k = t; k < QL; k += T) qtw[k] = A.qtwC[k];
+        __syncthreads();
+        inverse_from<GC, GC::P - 1, false, CtaSync, G, LE>(v, buf, qtw, tr, sync);
 
-            // ---- hop 1: unweight, round, round-off, two-digit chain per (row, column) from zero;
-            //      the carry-out goes to the next row. ----
-            const int sA0 = __ldg(A.sA + 2 * ar), sA1 = __ldg(A.sA + 2 * ar + 1);
-            const double ia0 = __ldg(A.iwA + 2 * ar), ia1 = __ldg(A.iwA + 2 * ar + 1);
+        // ---- hop 1: unweight, round, round-off, two-digit chain from zero; hop 2 for rows fed
+        //      from inside the tile (the carry-out of the lane above). Row G-1 publishes its
+        //      hop-1 and hop-2 carry-outs for the next tile (the wrap job: one column on). ----
+        const int slot = job + 1;
+        const double ia0 = __ldg(A.iwA + 2 * a), ia1 = __ldg(A.iwA + 2 * a + 1);
+        double lerr = 0.0;
+        float c2s[E];
 #pragma unroll
-            for (int i = 0; i < E; ++i) {
-                const int b = tr + TR * i;
-                const int sb = sB_of(b);
-                const double iwb = __ldg(A.iwB + b);
-                const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
-                const int s0 = o0 ? sA0 + sb - N : sA0 + sb, s1 = o1 ? sA1 + sb - N : sA1 + sb;
-                const bool w0 = s0 < A.rem, w1 = s1 < A.rem;  // digit of q + 1 bits
-                const double va = v[i].x * (ia0 * iwb) * (o0 ? 2.0 : 1.0);
-                const double vb = v[i].y * (ia1 * iwb) * (o1 ? 2.0 : 1.0);
-                long long ia, ib;
-                const double ra = round_shift(va, ia), rb = round_shift(vb, ib);
-                lerr = fmax(lerr, fmax(fabs(va - ra), fabs(vb - rb)));
-                double c;
-                x0s[i] = dsplit(ra, w0 ? iv1 : iv0, w0 ? pw1 : pw0, c);
-                x1s[i] = dsplit(rb + c, w1 ? iv1 : iv0, w1 ? pw1 : pw0, c);
-                carr[rg * C + b] = c;
+        for (int i = 0; i < E; ++i) {
+            const int b = tr + TR * i;
+            const double iwb = __ldg(A.iwB + b);
+            const uint32_t kd = digit_kind(b);
+            const bool w0 = kd & 1u, w1 = kd & 2u;
+            const double va = v[i].x * (ia0 * iwb) * ((kd & 4u) ? 2.0 : 1.0);
+            const double vb = v[i].y * (ia1 * iwb) * ((kd & 8u) ? 2.0 : 1.0);
+            long long ia, ib;
+            const double r0 = round_shift(va, ia), r1 = round_shift(vb, ib);
+            lerr = fmax(lerr, fmax(fabs(va - r0), fabs(vb - r1)));
+            double c, c1;
+            double x0 = dsplit_e(r0, A.q + w0, c);
+            double x1 = dsplit_e(r1 + c, A.q + w1, c1);
+            const int col = wrap_job ? ((b + 1) & (C - 1)) : b;  // row R-1, column b feeds row 0, column b+1
+            if (ra == G - 1) A.carry[(size_t)slot * C + col] = c1;
+            const double cin = __shfl_up_sync(FULL, c1, 1, G);
+            double c2 = 0.0;
+            if (ra > 0) {
+                x0 = dsplit_e(x0 + cin, A.q + w0, c);
+                x1 = dsplit_e(x1 + c, A.q + w1, c2);
             }
-            // the block's round-off max: one shared atomic per warp
+            if (ra == G - 1) A.carry2[(size_t)slot * C + col] = (float)c2;
+            v[i] = make_double2(x0, x1);
+            c2s[i] = (float)c2;
+        }
+        // the tile's round-off max: one shared atomic per warp
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) lerr = fmax(lerr, __shfl_xor_sync(0xffffffffu, lerr, o));
-            if ((t & 31) == 0) atomicMax(&s_err, (unsigned long long)__double_as_longlong(lerr));
-            __syncthreads();
-            // ---- hop 2 for rows fed from inside the block ----
-            if (rg > 0) {
-#pragma unroll
-                for (int i = 0; i < E; ++i) {
-                    const int b = tr + TR * i;
-                    const int sb = sB_of(b);
-                    const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
-                    const int s0 = o0 ? sA0 + sb - N : sA0 + sb, s1 = o1 ? sA1 + sb - N : sA1 + sb;
-                    const bool w0 = s0 < A.rem, w1 = s1 < A.rem;
-                    double c;
-                    x0s[i] = dsplit(x0s[i] + carr[(rg - 1) * C + b], w0 ? iv1 : iv0, w0 ? pw1 : pw0, c);
-                    x1s[i] = dsplit(x1s[i] + c, w1 ? iv1 : iv0, w1 ? pw1 : pw0, c);
-                    carr2[rg * C + b] = c;
-                }
-            }
-            if (ph == 0) {
-                // row R-1, column b feeds row 0, column b+1; column C-1 wraps to digit 0
-                if (rg == G - 1) {
-#pragma unroll
-                    for (int i = 0; i < E; ++i) {
-                        const int b = tr + TR * i;
-                        hin[(b + 1) & (C - 1)] = carr[(G - 1) * C + b];
-                        hin2[(b + 1) & (C - 1)] = carr2[(G - 1) * C + b];
-                    }
-                }
-                __syncthreads();  // carry arrays read before phase 1 reloads the buffers
-                continue;
-            }
-            if (rg == G - 1) {
-#pragma unroll
-                for (int i = 0; i < E; ++i) {
-                    const int b = tr + TR * i;
-                    A.carry[(size_t)blk * C + b] = carr[(G - 1) * C + b];
-                    A.carry2[(size_t)blk * C + b] = (float)carr2[(G - 1) * C + b];
-                }
-                __threadfence();  // each writer orders its carry-out stores before the flag below
-            }
-            __syncthreads();
-            // ---- hop 3 for rows 2 .. G-1: the small second-digit carry of the row above ----
-            if (rg >= 2) {
-#pragma unroll
-                for (int i = 0; i < E; ++i) x0s[i] += carr2[(rg - 1) * C + tr + TR * i];
-            }
-            if (t == 0) {
-                __threadfence();
-                *reinterpret_cast<volatile unsigned*>(&A.flags[blk]) = ep + 1u;
+        for (int o = 16; o > 0; o >>= 1) lerr = fmax(lerr, __shfl_xor_sync(FULL, lerr, o));
+        if ((t & 31) == 0) atomicMax(&s_err, (unsigned long long)__double_as_longlong(lerr));
+        if (ra == G - 1) __threadfence();  // each publisher orders its carry stores before the flag
+        __syncthreads();
+        if (t == 0) {
+            *reinterpret_cast<volatile unsigned*>(&A.flags[slot]) = ep + 1u;
+            if (!wrap_job) {
                 const unsigned long long eb = s_err;
                 atomicMax(&A.ctl->err_max, eb);
                 atomicMax(&A.ctl->err_since, eb);
-                if (A.errlog) atomicMax(reinterpret_cast<unsigned int*>(A.errlog + (ep % (unsigned)A.errlog_len)),
-                                        __float_as_uint((float)__longlong_as_double((long long)eb)));
+                if (A.errlog)
+                    atomicMax(reinterpret_cast<unsigned int*>(A.errlog + (ep % (unsigned)A.errlog_len)),
+                              __float_as_uint((float)__longlong_as_double((long long)eb)));
             }
-            // The carry arrays are read: each row may now reuse its exchange buffer, and rows
-            // 2 .. G-1 go on to the forward FFT. Row 0 waits for the previous block's carry-outs
-            // (hop 2 and 3 from outside the block); row 1 waits for row 0's hop-2 carry-outs,
-            // which pass through `late` (outside the exchange buffers).
-            __syncthreads();
-            if constexpr (TR >= 32) {
-                if (rg == 0) {
-                    if (t == 0 && blk > 0) wait_flag(&A.flags[blk - 1], ep + 1u, A.ctl, kSpinLimit);
-                    NamedSync{1u, (unsigned)TR}();
-                }
-            } else {
-                if (t == 0 && blk > 0) wait_flag(&A.flags[blk - 1], ep + 1u, A.ctl, kSpinLimit);
-                __syncthreads();
-            }
-            // ---- hop 2 and 3 for the block's first row: previous block's last row, or the wrap ----
-            if (rg == 0) {
+        }
+        if (wrap_job) return;
+        // ---- the tile's first row: hops 2 and 3 from the previous tile's last row (or the wrap) ----
+        if (t == 0) wait_flag(&A.flags[job], ep + 1u, A.ctl, A.spin_limit);
+        __syncthreads();
+        // (written without a branch on the row: every lane computes, the first row's lanes keep it)
+        const bool first = ra == 0;
+        const double* cprev = A.carry + (size_t)job * C;
+        const float* c2prev = A.carry2 + (size_t)job * C;
 #pragma unroll
-                for (int i = 0; i < E; ++i) {
-                    const int b = tr + TR * i;
-                    double cin = (blk > 0) ? __ldcg(A.carry + (size_t)(blk - 1) * C + b) : hin[b];
-                    if (a == 0 && b == 0) cin -= 2.0;  // the "- 2" of s^2 - 2 (digit 0)
-                    const int sb = sB_of(b);
-                    const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
-                    const int s0 = o0 ? sA0 + sb - N : sA0 + sb, s1 = o1 ? sA1 + sb - N : sA1 + sb;
-                    const bool w0 = s0 < A.rem, w1 = s1 < A.rem;
-                    double c;
-                    x0s[i] = dsplit(x0s[i] + cin, w0 ? iv1 : iv0, w0 ? pw1 : pw0, c);
-                    x1s[i] = dsplit(x1s[i] + c, w1 ? iv1 : iv0, w1 ? pw1 : pw0, c);
-                    late[b] = c;
-                    x0s[i] += (blk > 0) ? (double)__ldcg(A.carry2 + (size_t)(blk - 1) * C + b) : hin2[b];
-                }
-            }
-            if constexpr (TR >= 32) {
-                if (rg == 0) {
-                    __threadfence_block();
-                    NamedSync{(unsigned)G + 1u, 2u * TR}.arrive();
-                } else if (rg == 1) {
-                    NamedSync{(unsigned)G + 1u, 2u * TR}();
-                }
-            } else {
-                __syncthreads();
-            }
-            // ---- hop 3 for row 1 ----
-            if (rg == 1) {
+        for (int i = 0; i < E; ++i) {
+            const int b = tr + TR * i;
+            const uint32_t kd = digit_kind(b);
+            const bool w0 = kd & 1u, w1 = kd & 2u;
+            double cin = first ? __ldcg(cprev + b) : 0.0;
+            if (a == 0 && b == 0) cin -= 2.0;  // the "- 2" of s^2 - 2 (digit 0)
+            const float cin2 = first ? __ldcg(c2prev + b) : 0.f;
+            double c, c2;
+            const double x0 = dsplit_e(v[i].x + cin, A.q + w0, c);
+            const double x1 = dsplit_e(v[i].y + c, A.q + w1, c2);
+            // ---- hop 3: the hop-2 carry-out of the row above (the previous tile's for row 0) ----
+            const float up = __shfl_up_sync(FULL, first ? (float)c2 : c2s[i], 1, G);
+            v[i] = first ? make_double2(x0 + (double)cin2, x1) : make_double2(v[i].x + (double)up, v[i].y);
+        }
+        if (MODE == LARGE_FINAL || A.dump) {
 #pragma unroll
-                for (int i = 0; i < E; ++i) x0s[i] += late[tr + TR * i];
-            }
-            if (MODE == LARGE_FINAL || A.dump) {
-#pragma unroll
-                for (int i = 0; i < E; ++i) {
-                    const int b = tr + TR * i;
-                    const size_t m = (size_t)a + (size_t)R * b;
-                    *reinterpret_cast<int2*>(A.digits + 2 * m) =
-                        make_int2(__double2int_rn(x0s[i]), __double2int_rn(x1s[i]));
-                }
+            for (int i = 0; i < E; ++i) {
+                const size_t m = (size_t)a + (size_t)R * (tr + TR * i);
+                *reinterpret_cast<int2*>(A.digits + 2 * m) = make_int2(__double2int_rn(v[i].x), __double2int_rn(v[i].y));
             }
         }
         if constexpr (MODE == LARGE_FINAL) return;
     }
 
     // ---- weight, forward row FFT, store ----
-    const int sA0 = __ldg(A.sA + 2 * a), sA1 = __ldg(A.sA + 2 * a + 1);
     const double wa0 = __ldg(A.wA + 2 * a), wa1 = __ldg(A.wA + 2 * a + 1);
 #pragma unroll
     for (int i = 0; i < E; ++i) {
-        const int b = tr + TR * i;
-        const int sb = sB_of(b);
-        const double wb = __ldg(A.wB + b);
-        const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
-        v[i].x = x0s[i] * (wa0 * wb) * (o0 ? 0.5 : 1.0);
-        v[i].y = x1s[i] * (wa1 * wb) * (o1 ? 0.5 : 1.0);
+        const double wb = __ldg(A.wB + tr + TR * i);
+        const uint32_t kd = digit_kind(tr + TR * i);
+        v[i].x *= (wa0 * wb) * ((kd & 4u) ? 0.5 : 1.0);
+        v[i].y *= (wa1 * wb) * ((kd & 8u) ? 0.5 : 1.0);
     }
-    forward_from<GC, 0>(v, buf, qtw, tr, gsync);
+    forward_from<GC, 0, CtaSync, G, LE>(v, buf, qtw, tr, sync);
+    if (MODE == LARGE_ITER && job == A.nblocks - 1) {
+        // rows R-G .. R-1 are the wrap job's input: wait (bounded) until it has read them
+        if (t == 0) wait_flag(&A.flags[0], ep + 1u, A.ctl, A.spin_limit);
+        __syncthreads();
+    }
 #pragma unroll
-    for (int j = 0; j < E; ++j) buf[phys(tr * E + j)] = v[j];
-    if (MODE == LARGE_ITER && blk == A.nblocks - 1 && t == 0) {
-        // rows R-G .. R-1 are block 0's wrap-around input: wait (bounded) until it has read them
-        wait_flag(&A.ctl->halo_read, ep + 1u, A.ctl, kSpinLimit);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < G * C / T; ++r) {
-        const int qq = t + T * r, pos = qq / G, ra = qq % G;
-        A.V[(size_t)pos * R + a0 + ra] = bufs[ra * RS + phys(pos)];
-    }
+    for (int j = 0; j < E; ++j) __stcg(A.V + (size_t)(tr * E + j) * R + a, v[j]);
 }
 
 // Column pass: one block owns the column pair (c, C-c), one half of its threads per column; the
@@ -405,7 +320,7 @@ __global__ void __launch_bounds__(2 * (1 << LOG_R) / (1 << kLargeLogE), (LOG_R <
 template <int LOG_C, int G>
 static size_t row_smem() {
     using GC = SmallG<LOG_C, large_row_log_e(LOG_C, G), TW_FULL>;
-    return sizeof(double2) * (G * (GC::PAD + 1) + twiddle_table_len<GC>()) + sizeof(double) * GC::M;
+    return sizeof(double2) * (large_row_slots(LOG_C, G) + twiddle_table_len<GC>());
 }
 
 template <int LOG_R>
@@ -434,9 +349,12 @@ static cudaError_t col_attr() {
                                 (int)col_smem<LOG_R>());
 }
 
+// INIT: one block per tile. ITER / FINAL: one block more, for the wrap-around job (grid == 0), or
+// `grid` blocks.
 template <int LOG_C, int G, int MODE>
-static cudaError_t row_t(const LargeArgs& a, cudaStream_t st) {
-    large_row<LOG_C, G, MODE><<<a.nblocks, large_row_threads(LOG_C, G), row_smem<LOG_C, G>(), st>>>(a);
+static cudaError_t row_t(const LargeArgs& a, cudaStream_t st, int grid) {
+    if (grid <= 0) grid = a.nblocks + (MODE == LARGE_INIT ? 0 : 1);
+    large_row<LOG_C, G, MODE><<<grid, large_row_threads(LOG_C, G), row_smem<LOG_C, G>(), st>>>(a);
     return cudaGetLastError();
 }
 
@@ -449,22 +367,12 @@ static cudaError_t col_t(const LargeArgs& a, cudaStream_t st) {
 // Opts the kernels of one geometry into their dynamic shared memory (once per device, before
 // any launch or graph capture).
 cudaError_t configure_large(int log_c, int g, int log_r) {
-    cudaError_t e = cudaSuccess;
-    if (!large_rows_supported(log_c, g)) return cudaErrorInvalidValue;
-    const int key = 16 * log_c + g;
-    switch (key) {
-        case 16 * 6 + 4: e = row_attrs<6, 4>(); break;
-        case 16 * 7 + 4: e = row_attrs<7, 4>(); break;
-        case 16 * 8 + 4: e = row_attrs<8, 4>(); break;
-        case 16 * 9 + 4: e = row_attrs<9, 4>(); break;
-        case 16 * 10 + 4: e = row_attrs<10, 4>(); break;
-        case 16 * 11 + 4: e = row_attrs<11, 4>(); break;
-        case 16 * 8 + 2: e = row_attrs<8, 2>(); break;
-        case 16 * 9 + 2: e = row_attrs<9, 2>(); break;
-        case 16 * 10 + 2: e = row_attrs<10, 2>(); break;
-        case 16 * 11 + 2: e = row_attrs<11, 2>(); break;
-        case 16 * 9 + 8: e = row_attrs<9, 8>(); break;
-        case 16 * 10 + 8: e = row_attrs<10, 8>(); break;
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (16 * log_c + g) {
+#define LLG_ROW_ATTRS(LC, GG) \
+    case 16 * LC + GG: e = row_attrs<LC, GG>(); break;
+        LLG_ROW_SHAPES(LLG_ROW_ATTRS)
+#undef LLG_ROW_ATTRS
         default: return cudaErrorInvalidValue;
     }
     if (e) return e;
@@ -480,29 +388,21 @@ cudaError_t configure_large(int log_c, int g, int log_r) {
 }
 
 template <int MODE>
-static cudaError_t row_mode(int log_c, int g, const LargeArgs& a, cudaStream_t st) {
+static cudaError_t row_mode(int log_c, int g, const LargeArgs& a, cudaStream_t st, int grid) {
     switch (16 * log_c + g) {
-        case 16 * 6 + 4: return row_t<6, 4, MODE>(a, st);
-        case 16 * 7 + 4: return row_t<7, 4, MODE>(a, st);
-        case 16 * 8 + 4: return row_t<8, 4, MODE>(a, st);
-        case 16 * 9 + 4: return row_t<9, 4, MODE>(a, st);
-        case 16 * 10 + 4: return row_t<10, 4, MODE>(a, st);
-        case 16 * 11 + 4: return row_t<11, 4, MODE>(a, st);
-        case 16 * 8 + 2: return row_t<8, 2, MODE>(a, st);
-        case 16 * 9 + 2: return row_t<9, 2, MODE>(a, st);
-        case 16 * 10 + 2: return row_t<10, 2, MODE>(a, st);
-        case 16 * 11 + 2: return row_t<11, 2, MODE>(a, st);
-        case 16 * 9 + 8: return row_t<9, 8, MODE>(a, st);
-        case 16 * 10 + 8: return row_t<10, 8, MODE>(a, st);
+#define LLG_ROW_LAUNCH(LC, GG) \
+    case 16 * LC + GG: return row_t<LC, GG, MODE>(a, st, grid);
+        LLG_ROW_SHAPES(LLG_ROW_LAUNCH)
+#undef LLG_ROW_LAUNCH
         default: return cudaErrorInvalidValue;
     }
 }
 
-cudaError_t launch_large_row(int log_c, int g, int mode, const LargeArgs& a, cudaStream_t st) {
+cudaError_t launch_large_row(int log_c, int g, int mode, const LargeArgs& a, cudaStream_t st, int grid) {
     switch (mode) {
-        case LARGE_INIT: return row_mode<LARGE_INIT>(log_c, g, a, st);
-        case LARGE_ITER: return row_mode<LARGE_ITER>(log_c, g, a, st);
-        case LARGE_FINAL: return row_mode<LARGE_FINAL>(log_c, g, a, st);
+        case LARGE_INIT: return row_mode<LARGE_INIT>(log_c, g, a, st, grid);
+        case LARGE_ITER: return row_mode<LARGE_ITER>(log_c, g, a, st, grid);
+        case LARGE_FINAL: return row_mode<LARGE_FINAL>(log_c, g, a, st, grid);
         default: return cudaErrorInvalidValue;
     }
 }

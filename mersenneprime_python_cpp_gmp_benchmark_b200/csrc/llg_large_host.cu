@@ -113,7 +113,7 @@ bool large_split_supported(int log_n, int log_c, int rows) {
 
 LargeTest::~LargeTest() {
     if (exec) cudaGraphExecDestroy(exec);
-    void* ptrs[] = {V, carry, carry2, halo, ctl, flags, digits, errlog, qtwC, qtwR, tw1, tw2, pos_of_c, wA, iwA, sA, wB, iwB, sB};
+    void* ptrs[] = {V, carry, carry2, ctl, flags, digits, errlog, qtwC, qtwR, tw1, tw2, pos_of_c, wA, iwA, sA, wB, iwB, sB};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -165,13 +165,13 @@ cudaError_t LargeTest::init(uint64_t p_, int log_n, int log_c, int rows_) {
     if ((e = upload(&sB, hsB))) return e;
     // state
     if ((e = cudaMalloc(&V, M * sizeof(double2)))) return e;
-    if ((e = cudaMalloc(&carry, (size_t)nblocks * C * sizeof(double)))) return e;
-    if ((e = cudaMalloc(&carry2, (size_t)nblocks * C * sizeof(float)))) return e;
-    if ((e = cudaMalloc(&halo, (size_t)C * 2 * sizeof(double)))) return e;
+    // carry slots and flags: one per tile plus slot 0 for the wrap-around job
+    if ((e = cudaMalloc(&carry, (size_t)(nblocks + 1) * C * sizeof(double)))) return e;
+    if ((e = cudaMalloc(&carry2, (size_t)(nblocks + 1) * C * sizeof(float)))) return e;
     if ((e = cudaMalloc(&ctl, sizeof(LargeCtl)))) return e;
     if ((e = cudaMemset(ctl, 0, sizeof(LargeCtl)))) return e;
-    if ((e = cudaMalloc(&flags, (size_t)nblocks * sizeof(unsigned)))) return e;
-    if ((e = cudaMemset(flags, 0, (size_t)nblocks * sizeof(unsigned)))) return e;
+    if ((e = cudaMalloc(&flags, (size_t)(nblocks + 1) * sizeof(unsigned)))) return e;
+    if ((e = cudaMemset(flags, 0, (size_t)(nblocks + 1) * sizeof(unsigned)))) return e;
     if ((e = cudaMalloc(&digits, N * sizeof(int)))) return e;
     errlog_len = 1 << 16;
     if ((e = cudaMalloc(&errlog, errlog_len * sizeof(float)))) return e;
@@ -193,12 +193,12 @@ cudaError_t LargeTest::init(uint64_t p_, int log_n, int log_c, int rows_) {
     A.sB = sB;
     A.carry = carry;
     A.carry2 = carry2;
-    A.halo = halo;
     A.ctl = ctl;
     A.flags = flags;
     A.digits = digits;
     A.errlog = errlog;
     A.errlog_len = errlog_len;
+    A.spin_limit = kSpinLimit;
     A.dump = 0;
     A.tw_shift = s;
     A.C = C;
@@ -213,8 +213,13 @@ cudaError_t LargeTest::init(uint64_t p_, int log_n, int log_c, int rows_) {
 cudaError_t LargeTest::start(const std::vector<int>& d, cudaStream_t st) {
     cudaError_t e;
     if ((e = cudaMemcpyAsync(digits, d.data(), d.size() * sizeof(int), cudaMemcpyHostToDevice, st))) return e;
+    return start_device(st);
+}
+
+cudaError_t LargeTest::start_device(cudaStream_t st) {
+    cudaError_t e;
     if ((e = cudaMemsetAsync(ctl, 0, sizeof(LargeCtl), st))) return e;
-    if ((e = cudaMemsetAsync(flags, 0, (size_t)nblocks * sizeof(unsigned), st))) return e;
+    if ((e = cudaMemsetAsync(flags, 0, (size_t)(nblocks + 1) * sizeof(unsigned), st))) return e;
     if ((e = cudaMemsetAsync(errlog, 0, errlog_len * sizeof(float), st))) return e;
     if ((e = launch_large_row(logC, rows, LARGE_INIT, args, st))) return e;
     if ((e = launch_large_col(logR, args, st))) return e;
@@ -266,8 +271,7 @@ cudaError_t LargeTest::final_pass(cudaStream_t st) {
     cudaError_t e;
     if ((e = launch_large_row(logC, rows, LARGE_FINAL, args, st))) return e;
     // the squarings may resume from this state at the same epoch: clear the flags FINAL set
-    if ((e = cudaMemsetAsync(&ctl->halo_read, 0, sizeof(unsigned), st))) return e;
-    return cudaMemsetAsync(flags, 0, (size_t)nblocks * sizeof(unsigned), st);
+    return cudaMemsetAsync(flags, 0, (size_t)(nblocks + 1) * sizeof(unsigned), st);
 }
 
 cudaError_t LargeTest::finish(cudaStream_t st, std::vector<int>& out) {
@@ -276,6 +280,22 @@ cudaError_t LargeTest::finish(cudaStream_t st, std::vector<int>& out) {
     out.resize(2 * M);
     if ((e = cudaMemcpyAsync(out.data(), digits, 2 * M * sizeof(int), cudaMemcpyDeviceToHost, st))) return e;
     return cudaStreamSynchronize(st);
+}
+
+cudaError_t LargeTest::diag_withhold_wrap(unsigned long long spin_limit, cudaStream_t st, bool& timed_out) {
+    LargeCtl h;
+    cudaError_t e = read_ctl(h, st);
+    if (e) return e;
+    // tickets start at 1: ticket 0, the wrap-around job, is never handed out, so tile 0 and the
+    // last tile wait for its flag until their limit runs out; every index stays that of a tile
+    const unsigned one = 1u;
+    if ((e = cudaMemcpyAsync(&ctl->ticket[h.epoch & 1u], &one, sizeof one, cudaMemcpyHostToDevice, st))) return e;
+    LargeArgs a = args;
+    a.spin_limit = spin_limit;
+    if ((e = launch_large_row(logC, rows, LARGE_ITER, a, st, nblocks))) return e;
+    if ((e = read_ctl(h, st))) return e;
+    timed_out = h.timeout != 0;
+    return cudaSuccess;
 }
 
 cudaError_t LargeTest::read_ctl(LargeCtl& h, cudaStream_t st) {
@@ -521,6 +541,11 @@ cudaError_t NttLargeTest::init(uint64_t p_, int log_n) {
 cudaError_t NttLargeTest::start(const std::vector<int>& d, cudaStream_t st) {
     cudaError_t e;
     if ((e = cudaMemcpyAsync(digits, d.data(), d.size() * sizeof(int), cudaMemcpyHostToDevice, st))) return e;
+    return start_device(st);
+}
+
+cudaError_t NttLargeTest::start_device(cudaStream_t st) {
+    cudaError_t e;
     if ((e = cudaMemsetAsync(ctl, 0, sizeof(LargeCtl), st))) return e;
     if ((e = cudaMemsetAsync(args.flags, 0, (size_t)nblocks * sizeof(unsigned), st))) return e;
     if ((e = launch_ntt_row(logC, LARGE_INIT, args, st))) return e;

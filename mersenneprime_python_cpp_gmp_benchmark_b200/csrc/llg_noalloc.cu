@@ -65,7 +65,7 @@ struct TableKey {
 TableKey g_tables_for[kMaxDevices];
 
 struct Layout {
-    size_t V, carry, carry2, halo, ctl, flags, qtwC, qtwR, tw1, tw2, pos_of_c, wA, iwA, sA, wB, iwB, sB, end;
+    size_t V, carry, carry2, ctl, flags, qtwC, qtwR, tw1, tw2, pos_of_c, wA, iwA, sA, wB, iwB, sB, end;
 };
 
 size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -76,11 +76,10 @@ Layout layout(int logN, int logC, int logR, int s) {
     Layout L;
     size_t o = 0;
     L.V = o; o = up256(o + M * sizeof(double2));
-    L.carry = o; o = up256(o + nblocks * C * sizeof(double));
-    L.carry2 = o; o = up256(o + nblocks * C * sizeof(float));
-    L.halo = o; o = up256(o + C * 2 * sizeof(double));
+    L.carry = o; o = up256(o + (nblocks + 1) * C * sizeof(double));  // slot 0: the wrap-around job
+    L.carry2 = o; o = up256(o + (nblocks + 1) * C * sizeof(float));
     L.ctl = o; o = up256(o + sizeof(LargeCtl));
-    L.flags = o; o = up256(o + nblocks * sizeof(unsigned));
+    L.flags = o; o = up256(o + (nblocks + 1) * sizeof(unsigned));
     L.qtwC = o; o = up256(o + qpad_len((uint32_t)C) * sizeof(double2));
     L.qtwR = o; o = up256(o + qpad_len((uint32_t)(R / 4)) * sizeof(double2));
     L.tw1 = o; o = up256(o + ((size_t)1 << s) * sizeof(double2));
@@ -223,12 +222,12 @@ extern "C" int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* 
     A.sB = reinterpret_cast<const int*>(base + L.sB);
     A.carry = reinterpret_cast<double*>(base + L.carry);
     A.carry2 = reinterpret_cast<float*>(base + L.carry2);
-    A.halo = reinterpret_cast<double*>(base + L.halo);
     A.ctl = reinterpret_cast<LargeCtl*>(base + L.ctl);
     A.flags = reinterpret_cast<unsigned*>(base + L.flags);
     A.digits = digits_out;
     A.errlog = nullptr;
     A.errlog_len = 1;
+    A.spin_limit = kSpinLimit;
     A.dump = 0;
     A.tw_shift = s;
     A.C = C;
@@ -250,7 +249,7 @@ extern "C" int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* 
     if ((e = cudaMemcpyAsync(digits_out, &four, sizeof four, cudaMemcpyHostToDevice, st)) != cudaSuccess)
         return fail_enqueued("writing s_0", e);
     if ((e = cudaMemsetAsync(A.ctl, 0, sizeof(LargeCtl), st)) != cudaSuccess) return fail_enqueued("clearing the control block", e);
-    if ((e = cudaMemsetAsync(A.flags, 0, (size_t)A.nblocks * sizeof(unsigned), st)) != cudaSuccess)
+    if ((e = cudaMemsetAsync(A.flags, 0, (size_t)(A.nblocks + 1) * sizeof(unsigned), st)) != cudaSuccess)
         return fail_enqueued("clearing the carry flags", e);
     const int G = large_rows_per_block(logC);
     if ((e = launch_large_row(logC, G, LARGE_INIT, A, st)) != cudaSuccess) return fail_enqueued("row pass launch", e);

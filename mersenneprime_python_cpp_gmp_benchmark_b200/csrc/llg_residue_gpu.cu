@@ -9,11 +9,14 @@
 //      per-chunk carry maps ({-1,0,1} -> {-1,0,1}, composed in one block);
 //   3. the bits at and above p fold back into bit 0 (2^p == 1), by one thread with early exit;
 //   4. 2^p - 1 (all ones) is the canonical zero.
+// The inverse direction, digits_from_words, forms the digits of a residue at any length on the
+// GPU (a test resumed or moved to a longer transform from a residue).
 #include <cuda_runtime.h>
 
 #include <cstdint>
 
 #include "../../include/llgpu.h"
+#include "llg_internal.h"
 
 namespace llg {
 
@@ -28,7 +31,8 @@ __device__ __forceinline__ uint64_t first_digit(uint64_t w, uint64_t p, uint64_t
     return w == 0 ? 0 : ((64 * w - 1) * n) / p + 1;
 }
 
-__device__ __int128 word_sum(uint64_t w, const int32_t* __restrict__ d, uint64_t p, uint64_t n) {
+template <class D>
+__device__ __int128 word_sum(uint64_t w, const D* __restrict__ d, uint64_t p, uint64_t n) {
     uint64_t j0 = first_digit(w, p, n), j1 = first_digit(w + 1, p, n);
     if (j0 > n) j0 = n;
     if (j1 > n) j1 = n;
@@ -183,7 +187,151 @@ __global__ void check_kernel(const uint64_t* __restrict__ F, uint64_t nw, uint64
     if (__any_sync(0xffffffffu, nonzero) && (threadIdx.x & 31) == 0) atomicOr(&flags[1], 1u);
 }
 
+// Bits [s, s + b) of the p-bit residue in `words` (b <= 62, s + b <= p).
+__device__ __forceinline__ uint64_t residue_bits(const uint64_t* __restrict__ words, uint64_t s, int b) {
+    const uint64_t w = s >> 6;
+    const int sh = (int)(s & 63);
+    unsigned __int128 x = words[w] >> sh;
+    if (sh + b > 64) x |= (unsigned __int128)words[w + 1] << (64 - sh);
+    return (uint64_t)x & ((1ull << b) - 1ull);
+}
+
+// Digit j of s at length n, within one of balanced: raw bits r_j = bits [ceil(jp/n), ceil((j+1)p/n))
+// of s; x_j = r_j - 2^b_j [r_j >= 2^(b_j - 1)] + [r_{j-1} >= 2^(b_{j-1} - 1)] (j - 1 of digit 0 is
+// digit n - 1: 2^p == 1). Every carry comes from one digit's own top bit, so no chain forms:
+// sum_j x_j 2^ceil(jp/n) == s mod 2^p - 1 and |x_j| <= 2^(b_j - 1).
+__global__ void digits_from_words_kernel(const uint64_t* __restrict__ words, uint64_t p, uint64_t n,
+                                         int32_t* __restrict__ digits) {
+    const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const uint64_t jm = (j == 0) ? n - 1 : j - 1;
+    const uint64_t s0 = off_of(j, p, n), s1 = off_of(j + 1, p, n), sm = off_of(jm, p, n), sm1 = off_of(jm + 1, p, n);
+    const int b = (int)(s1 - s0), bm = (int)(sm1 - sm);
+    const long long r = (long long)residue_bits(words, s0, b);
+    const long long rm = (long long)residue_bits(words, sm, bm);
+    const long long hi = (r >> (b - 1)) & 1, him = (rm >> (bm - 1)) & 1;
+    digits[j] = (int32_t)(r - (hi << b) + him);
+}
+
+// One block per exponent of a whole-test batch (digits: cnt x n int64, natural order; the batch's
+// job list gives p): the same rebuild as the kernels above, every step inside the block with the
+// p-bit number in shared memory. Words and their carry-outs; the +-1 chains by per-thread segment
+// maps and a block scan; the fold above p by one thread; the all-ones / zero check. Out per
+// exponent: res64, flags (bit 0: residue zero, bit 1: the fold did not settle) and, with words
+// non-null, the ceil(p/64) words at word_off[i].
+constexpr int kBatchThreads = 256;
+__global__ void __launch_bounds__(kBatchThreads) rebuild_batch_kernel(
+    const int64_t* __restrict__ digits, const SmallJob* __restrict__ jobs, uint32_t n, uint64_t* __restrict__ res64,
+    int32_t* __restrict__ flags, uint64_t* __restrict__ words, const uint64_t* __restrict__ word_off, uint64_t nw_cap) {
+    extern __shared__ uint64_t F[];  // nw_cap words, then nw_cap carry-outs (int8)
+    int8_t* e = reinterpret_cast<int8_t*>(F + nw_cap);
+    __shared__ uint8_t agg[kBatchThreads];
+    __shared__ long long s_top;
+    __shared__ int s_top_carry, s_status, s_ones, s_nonzero;
+    const int t = threadIdx.x, i = blockIdx.x;
+    const uint64_t p = jobs[i].p, nw = (p + 63) / 64;
+    const int64_t* d = digits + (size_t)i * n;
+    if (t == 0) {
+        s_status = 0;
+        s_ones = 1;
+        s_nonzero = 0;
+    }
+    for (uint64_t w = t; w < nw; w += kBatchThreads) {
+        const __int128 sw = word_sum(w, d, p, n);
+        const __int128 cin = (w > 0) ? (word_sum(w - 1, d, p, n) >> 64) : (__int128)0;
+        const __int128 tw = (__int128)(unsigned __int128)(uint64_t)sw + cin;
+        F[w] = (uint64_t)tw;
+        e[w] = (int8_t)(tw >> 64);
+        if (w == nw - 1) s_top = (long long)(sw >> 64);
+    }
+    __syncthreads();
+    // the +-1 chains: map of each thread's segment of words, inclusive scan, then the carries in
+    const uint64_t per = (nw + kBatchThreads - 1) / kBatchThreads;
+    const uint64_t w0 = t * per, w1 = (w0 + per < nw) ? w0 + per : nw;
+    uint8_t f = 0x24;  // identity map
+    for (uint64_t w = w0; w < w1; ++w) {
+        uint8_t m = 0;
+        for (int k = 0; k < 3; ++k) m |= (uint8_t)((word_carry(F[w], e[w], k - 1) + 1) << (2 * k));
+        f = compose(f, m);
+    }
+    agg[t] = f;
+    __syncthreads();
+    for (int sh = 1; sh < kBatchThreads; sh <<= 1) {
+        const uint8_t mine = agg[t];
+        const uint8_t left = (t >= sh) ? agg[t - sh] : (uint8_t)0x24;
+        __syncthreads();
+        agg[t] = compose(left, mine);
+        __syncthreads();
+    }
+    int x = (t == 0) ? 0 : apply_map(agg[t - 1], 0);
+    for (uint64_t w = w0; w < w1; ++w) {
+        const uint64_t u = F[w];
+        const int xo = word_carry(u, e[w], x);
+        F[w] = u + (uint64_t)(long long)x;
+        x = xo;
+    }
+    if (t == kBatchThreads - 1) s_top_carry = apply_map(agg[t], 0);
+    __syncthreads();
+    if (t == 0) {  // fold everything at and above bit p into bit 0
+        __int128 h = take_high(F, nw, p, s_top + s_top_carry);
+        for (int guard = 0; h != 0; ++guard) {
+            if (guard > 8) {
+                s_status = 1;
+                break;
+            }
+            const long long over = add_low(F, nw, h);
+            h = take_high(F, nw, p, over);
+        }
+    }
+    __syncthreads();
+    const unsigned r = (unsigned)(p % 64);
+    bool ones = true, nonzero = false;
+    for (uint64_t w = t; w < nw; w += kBatchThreads) {
+        const uint64_t full = (w == nw - 1 && r) ? ((1ull << r) - 1ull) : ~0ull;
+        ones = ones && F[w] == full;
+        nonzero = nonzero || F[w] != 0;
+    }
+    if (!ones) atomicAnd(&s_ones, 0);
+    if (nonzero) atomicOr(&s_nonzero, 1);
+    __syncthreads();
+    const bool zero = s_ones || !s_nonzero;  // 2^p - 1 (all ones) is the canonical zero
+    if (t == 0) {
+        res64[i] = zero ? 0 : F[0];
+        flags[i] = (zero ? 1 : 0) | (s_status ? 2 : 0);
+    }
+    if (words) {
+        uint64_t* out = words + word_off[i];
+        for (uint64_t w = t; w < nw; w += kBatchThreads) out[w] = zero ? 0 : F[w];
+    }
+}
+
 }  // namespace
+
+cudaError_t rebuild_batch(const int64_t* d_digits, const SmallJob* d_jobs, int cnt, uint32_t n, uint64_t pmax,
+                          uint64_t* d_res64, int32_t* d_flags, uint64_t* d_words, const uint64_t* d_word_off,
+                          cudaStream_t st) {
+    if (cnt <= 0) return cudaSuccess;
+    const uint64_t nw_cap = (pmax + 63) / 64;
+    const size_t smem = nw_cap * (sizeof(uint64_t) + 1) + 16;
+    if (smem > 200 * 1024) return cudaErrorInvalidValue;
+    static PerDeviceOnce configured;
+    if (!configured.done()) {
+        const cudaError_t e = cudaFuncSetAttribute(rebuild_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   200 * 1024);
+        if (e != cudaSuccess) return e;
+        configured.mark();
+    }
+    rebuild_batch_kernel<<<cnt, kBatchThreads, smem, st>>>(d_digits, d_jobs, n, d_res64, d_flags, d_words, d_word_off,
+                                                           nw_cap);
+    return cudaGetLastError();
+}
+
+cudaError_t digits_from_words(uint64_t p, uint64_t n, const uint64_t* d_words, int32_t* d_digits, cudaStream_t st) {
+    if (n == 0 || p < n || (p + n - 1) / n > 30) return cudaErrorInvalidValue;
+    const unsigned B = 256;
+    digits_from_words_kernel<<<(unsigned)((n + B - 1) / B), B, 0, st>>>(d_words, p, n, d_digits);
+    return cudaGetLastError();
+}
 
 }  // namespace llg
 

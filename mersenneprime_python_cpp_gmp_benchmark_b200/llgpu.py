@@ -53,6 +53,9 @@ def lib() -> ctypes.CDLL:
         L.llg_fft_length.argtypes = [u64, dbl]
         L.llg_fft_length.restype = u32
         L.llg_set_max_bpw.argtypes = [dbl]
+        L.llg_set_roundoff_limit.argtypes = [dbl]
+        L.llg_get_roundoff_limit.argtypes = []
+        L.llg_get_roundoff_limit.restype = dbl
         L.llg_get_max_bpw.restype = dbl
         L.llg_ntt_length.argtypes = [u64]
         L.llg_ntt_length.restype = u32
@@ -81,6 +84,8 @@ def lib() -> ctypes.CDLL:
         L.llg_test_time_passes.argtypes = [ctypes.c_void_p, u64, ctypes.c_void_p, P(ctypes.c_double),
                                            P(ctypes.c_double)]
         L.llg_test_destroy.argtypes = [ctypes.c_void_p]
+        L.llg_test_load.argtypes = [ctypes.c_void_p, P(u64), sz, u64, ctypes.c_void_p]
+        L.llg_test_diag_withhold_wrap.argtypes = [ctypes.c_void_p, u64, ctypes.c_void_p]
         L.llg_test_destroy.restype = None
         L.llg_batch_destroy.restype = None
         _lib = L
@@ -122,6 +127,15 @@ def fft_length(p, max_bpw=0.0):
 
 def ntt_length(p):
     return int(lib().llg_ntt_length(p))
+
+
+def set_roundoff_limit(limit):
+    """llg_set_roundoff_limit: the FP64 round-off bound above which a test is redone longer."""
+    _check(lib().llg_set_roundoff_limit(limit))
+
+
+def get_roundoff_limit():
+    return lib().llg_get_roundoff_limit()
 
 
 def set_large_split(log_n, log_c, rows=0):
@@ -302,6 +316,17 @@ class Test:
         if want_words:
             d["words"] = list(words)
         return d
+
+    def load(self, words, iters_done, stream=0):
+        """llg_test_load: the state becomes the residue `words` (ceil(p/64) limbs) after
+        `iters_done` squarings, and the next squaring starts."""
+        nw = nwords(self.p)
+        arr = (ctypes.c_uint64 * nw)(*words[:nw])
+        _check(lib().llg_test_load(self.h, arr, nw, iters_done, ctypes.c_void_p(stream or None)))
+
+    def diag_withhold_wrap(self, spin_limit, stream=0):
+        """llg_test_diag_withhold_wrap: one row pass whose waits must run out (raises LlgError)."""
+        _check(lib().llg_test_diag_withhold_wrap(self.h, spin_limit, ctypes.c_void_p(stream or None)))
 
     def time_passes(self, iters, stream=0):
         """`iters` squarings one pass at a time: (mean row-pass us, mean column-pass us)."""

@@ -261,3 +261,113 @@ def test_device_residue_rebuild_matches_host(gpu):
     for d in ([0] * n, [(1 << x) - 1 for x in bits], [-1] + [0] * (n - 1), [1 << 30] * n, [-(1 << 30)] * n):
         dd = torch.tensor(d, dtype=torch.int32, device="cuda")
         assert gpu.residue_from_digits_device(p, n, dd.data_ptr(), want_words=True) == gpu.residue_from_digits(p, n, d)
+
+
+# ---- state load, snapshot escalation and the bounded waits --------------------------------------
+
+@pytest.mark.parametrize("engine,n1,n2", [("fp64", 1 << 18, 1 << 18), ("fp64", 1 << 18, 1 << 19),
+                                           ("ntt", 1 << 18, 1 << 19), ("fp64", 1 << 19, 1 << 18)])
+def test_load_resumes_exactly(gpu, oracle, engine, n1, n2):
+    """llg_test_load: a residue read after k squarings at one length, re-digitised on the GPU at
+    the same, a longer or a shorter length (or from the other engine), resumes bit-exactly. p is
+    usable at both 2^18 and 2^19 (17.2 and 8.6 bits per digit)."""
+    p, k, m = _odd_candidate(4500000), 300, 200
+    a = gpu.Test(p, n1)
+    a.start()
+    a.iterate(k - 1)
+    w = a.read(want_words=True)["words"]
+    a.close()
+    b = gpu.Test(p, n2, engine)
+    b.load(w, k)
+    b.iterate(m - 1)
+    r = b.read(want_words=True)
+    b.close()
+    assert r["iters"] == k + m and r["status"] == 0
+    assert r["words"] == oracle.ll_gmp(p, k + m)[2]
+
+
+def test_corrupted_state_changes_res64(gpu):
+    """The exit-3 contract of the reference driver (PerfNumMultiCLL.py:123-129, 234) rests on a
+    wrong residue showing in res64: one flipped bit of an interim state, loaded and run on, ends at
+    a res64 different from the reference's; the unflipped state ends at the reference's."""
+    p, k, total = 1257787, 5000, 10000
+    want = int(load_json("trace_1257787.json")["res64"][0], 16)  # after 10^4 squarings
+    a = gpu.Test(p, 65536)
+    a.start()
+    a.iterate(k - 1)
+    w = a.read(want_words=True)["words"]
+    a.close()
+    for flip in (None, (1000, 17), (0, 0)):
+        words = list(w)
+        if flip:
+            words[flip[0]] ^= 1 << flip[1]
+        t = gpu.Test(p, 65536)
+        t.load(words, k)
+        t.iterate(total - k - 1)
+        r = t.read()
+        t.close()
+        assert r["iters"] == total
+        assert (r["res64"] == want) == (flip is None), flip
+
+
+def _later_chunk_exceeding(log, chunk):
+    """First chunk c >= 2 of the per-squaring round-off log whose worst value exceeds every earlier
+    chunk's, with the bound halfway between the two; None when the first chunk holds the maximum."""
+    run = max(log[1:chunk + 1])
+    for c in range(2, (len(log) - 1) // chunk + 1):
+        m = max(log[(c - 1) * chunk + 1:c * chunk + 1])
+        if m > run:
+            return c, (run + m) / 2
+        run = max(run, m)
+    return None
+
+
+def test_escalation_resumes_from_snapshot(gpu):
+    """A round-off abort in the middle of a two-pass run is redone from the last checkpoint at the
+    next length: escalations == 1 and the residue equals the exact NTT engine's. The round-off bound
+    is set between the worst round-off of the chunks of 4096 squarings before some chunk j >= 2 and
+    chunk j's own (read from the run's per-squaring log), so the checks before j pass and check j
+    fails; the engine's arithmetic is deterministic, so the run under llg_run sees the same
+    round-off. Exponents at ~19 bits per digit are tried until one's log has such a chunk."""
+    n, chunk, total = 65536, 4096, 60000
+    for p in (1257787, 1250003, 1245011, 1253513, 1239017, 1247509):
+        t = gpu.Test(p, n)
+        t.start()
+        t.iterate(total - 1)
+        log = t.errlog(total)  # log[e]: worst round-off of squaring e (e >= 1)
+        t.close()
+        found = _later_chunk_exceeding(log, chunk)
+        if found:
+            break
+    assert found, "no exponent had a later chunk above its earlier ones"
+    j, limit = found
+    k = j * chunk + 1000  # past the abort, inside the redone chunk's successor
+    old = gpu.get_roundoff_limit()
+    try:
+        gpu.set_roundoff_limit(limit)
+        r = gpu.run(p, iters=k, n=n, want_words=True)
+    finally:
+        gpu.set_roundoff_limit(old)
+    assert r["status"] == 0 and r["escalations"] == 1 and r["n"] > n, (p, r["n"], j, limit)
+    want = gpu.run(p, iters=k, engine="ntt", want_words=True)
+    assert r["words"] == want["words"]
+
+
+def test_withheld_wrap_times_out_and_engine_recovers(gpu, oracle):
+    """The failure path of the bounded device-side waits: one row pass whose wrap-around job is
+    withheld (its flag can never arrive) and whose waits give up after 1000 sleeps. The kernel
+    returns, the call reports LLG_E_TIMEOUT quickly, and a following normal run in the same process
+    is bit-exact."""
+    import time
+    p, n = 330017, 1 << 16
+    t = gpu.Test(p, n)
+    t.start()
+    t.iterate(9)
+    t0 = time.perf_counter()
+    with pytest.raises(gpu.LlgError) as e:
+        t.diag_withhold_wrap(1000)
+    assert e.value.code == 6  # LLG_E_TIMEOUT
+    assert time.perf_counter() - t0 < 10.0
+    t.close()
+    r = gpu.run(p, iters=100, n=n, want_words=True)
+    assert r["status"] == 0 and r["words"] == oracle.ll_gmp(p, 100)[2]
