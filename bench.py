@@ -15,7 +15,8 @@ Workloads (synthetic inputs: the exponents themselves, s_0 = 4; no dataset exist
           kernels bucketed by transform length. One step = every test run to completion.
           metric: tests/s. e2e: lucaslehmer_cuda.lucas_lehmer_batch() on the host list.
           batched_vs_plain: every prime p <= 10,001 one exponent per launch against one batched
-          launch, on the same GPU (device time, residues compared).
+          launch, on the same GPU (device time, residues compared). reference_gpu: the reference's
+          own cuda/ll_ntt.cu (compiled unchanged for sm_100a) on a sample of the range, same GPU.
   single  p = 1,257,787 (a Mersenne exponent) at N = 65536, the whole test on the FP64 and NTT
           engines: us per squaring, res64 every 10^4 squarings against the reference GMP trace,
           final residue zero, the round-off maximum and per-squaring log.
@@ -272,6 +273,8 @@ def bench_range(args, rank, world):
     }
     if rank == 0:
         line["batched_vs_plain"] = plain_vs_batched(llgpu)
+        if not getattr(args, "no_reference_gpu", False):
+            line["reference_gpu"] = reference_gpu_range()
     return line
 
 
@@ -646,6 +649,49 @@ def cpu_baseline_range(threads, budget_s=20.0):
     return out
 
 
+REF_GPU_DIR = os.path.join(ROOT, "oracle", "_ref", "gpu")
+_REF_GPU_CODE = r"""
+import json, sys, time
+sys.path.insert(0, sys.argv[1])
+import lucaslehmer_cuda as ref
+ps = json.loads(sys.argv[2])
+ref.lucas_lehmer_batch(ps[:2])  # context, tables
+t0 = time.perf_counter()
+out = ref.lucas_lehmer_batch(ps)
+wall = time.perf_counter() - t0
+print(json.dumps({"wall": wall, "rows": [[p, bool(r), s, res] for p, r, s, res in out]}))
+"""
+
+
+def reference_gpu_range(every=8, timeout=600):
+    """The reference's own GPU engine (its cuda/ll_ntt.cu compiled unchanged for sm_100a into
+    oracle/_ref/gpu/: one block per exponent, radix-2 Goldilocks NTT in shared memory) on every
+    `every`-th prime p <= 100001 on this GPU, in a subprocess (its module name is the product's).
+    Exponents below 64 are not taken by that kernel (the driver runs them on the CPU); the rest are
+    timed wall-clock around its lucas_lehmer_batch and their res64 checked against the golden."""
+    if not os.path.exists(REF_GPU_DIR):
+        return {"unavailable": "oracle/_ref/gpu not built (needs the reference's sources at build time)"}
+    ps = [p for p in sieve(2, RANGE_HI) if p >= 64]
+    sample = ps[every // 2::every]
+    r = subprocess.run([sys.executable, "-c", _REF_GPU_CODE, REF_GPU_DIR, json.dumps(sample)],
+                       capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        return {"unavailable": "reference GPU engine failed: " + (r.stderr.strip().splitlines() or ["?"])[-1][:200]}
+    doc = json.loads(r.stdout.strip().splitlines()[-1])
+    gold = {}
+    for line in open(os.path.join(ROOT, "tests", "golden", "range_100001.csv")):
+        if not line.startswith("#"):
+            f = line.strip().split(",")
+            gold[int(f[0])] = int(f[2], 16)
+    bad = [p for p, isp, sec, res in doc["rows"] if sec >= 0 and res != gold[p]]
+    taken = sum(1 for row in doc["rows"] if row[2] >= 0)
+    full = len(ps) / len(sample)
+    return {"value": round(len(sample) / doc["wall"], 3), "unit": "tests/s",
+            "sample": f"every {every}th prime 64 <= p <= 100001 ({len(sample)} tests, {taken} taken by the kernel), "
+                      f"{doc['wall']:.2f} s wall around lucas_lehmer_batch; the full range is ~{full:.1f}x the sample",
+            "res64_mismatches": len(bad), "build": "reference cuda/ll_ntt.cu unchanged, nvcc -O3 sm_100a"}
+
+
 def cpu_baseline_big_fft():
     """The reference's FFT engine (oracle/_ref) per squaring at p = 136,279,841, N = 2^23:
     fft_res64_after(p, 3) - fft_res64_after(p, 1), one thread, over the substitute FFT."""
@@ -653,7 +699,7 @@ def cpu_baseline_big_fft():
     ref = oracle.reference_module()
     if ref is None:
         return None
-    ref.fft_res64_after(1257787, 2)  # planning and table paths warmed
+    ref.fft_res64_after(BIG_P, 1)  # planning and tables of this length warmed
     t0 = time.perf_counter()
     ref.fft_res64_after(BIG_P, 1)
     t1 = time.perf_counter()
@@ -678,6 +724,8 @@ def main():
     ap.add_argument("--sweep-ntt-iters", type=int, default=20000, help="sweep: NTT squarings timed per prime")
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="range: leave out the timing of the reference's own GPU engine")
     ap.add_argument("--no-range", action="store_true",
                     help="big: leave out the range sub-record (the other half of the metric)")
     args = ap.parse_args()

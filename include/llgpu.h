@@ -129,7 +129,8 @@ void llg_batch_destroy(llg_batch* b);
  * back, exact residue; waits; the squarings may resume after it). llg_result.iters counts the
  * squarings done since s_0 (start's included);
  * llg_result.status is LLG_E_ROUNDOFF when the worst round-off exceeded 0.4 (no escalation here).
- * llg_test_errlog (FP64): per-squaring max round-off (ring of 65536 entries).
+ * llg_test_errlog (FP64): per-squaring max round-off (ring of 65536 entries; entry e is squaring
+ * e, from 1); it waits for the device first.
  * Replaces the iteration loop of lucas_lehmer_fft_raw(), lucaslehmer.cpp:281-311, for large p. */
 typedef struct llg_test llg_test;
 int llg_test_create(uint64_t p, uint32_t n, int engine, llg_test** out);

@@ -11,10 +11,13 @@
 #include <cstdlib>
 #include <cstring>
 #include <atomic>
+#include <chrono>
+#include <condition_variable>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
@@ -677,7 +680,7 @@ int run_large(int engine, const Item& item, llg_result& r, std::vector<uint64_t>
 // strict: a single-exponent call fails on an unsupported exponent; a batch marks it and goes on
 // (the reference's batch returns such exponents with seconds < 0, cuda/ll_ntt.cu:259-267).
 int make_batch(const uint64_t* ps, size_t count, uint64_t max_iters, int engine, uint32_t n_force,
-               bool strict, int flags, llg_batch** outb) {
+               bool strict, int flags, llg_batch** outb, const uint64_t* iters_each = nullptr) {
     if (engine != LLG_ENGINE_FP64 && engine != LLG_ENGINE_NTT) return fail(LLG_E_ARG, "unknown engine %d", engine);
     const bool ntt = engine == LLG_ENGINE_NTT;
     int dev;
@@ -697,7 +700,8 @@ int make_batch(const uint64_t* ps, size_t count, uint64_t max_iters, int engine,
         set_trivial(&b->out[i], p);
         if (p < 3 || p % 2 == 0) continue;  // decided without iterating (lucaslehmer.cpp:31-33)
         const uint64_t full = p - 2;
-        const uint64_t iters = (max_iters && max_iters < full) ? max_iters : full;
+        const uint64_t mi = iters_each ? iters_each[i] : max_iters;
+        const uint64_t iters = (mi && mi < full) ? mi : full;
         b->out[i].iters = iters;
         Item it{i, p, iters, 0, 0};
         if (p >= kWordMaxP) {
@@ -839,6 +843,116 @@ int run_sync(llg_batch* b) {
     return collect_batch(b);
 }
 
+// ---- single-exponent calls from many host threads share batches ------------------------------
+// The reference's driver tests one exponent per call from a thread pool (PerfNumMultiCLL.py:34-42,
+// 174-193). llg_run calls whose length is a whole-test length join a per-device pool instead of
+// each making its own one-block launch: the first caller of a round leads it -- it waits
+// kGatherWindow for the calls arriving meanwhile, takes every pending request, runs them as one
+// batch (one launch per transform length), hands each caller its result and wakes it; a request
+// that arrived during the round leads the next one. The window is short while callers come one at
+// a time (the previous round held one request) and longer once several call at once.
+constexpr auto kGatherWindow = std::chrono::microseconds(150);
+constexpr auto kGatherWindowAlone = std::chrono::microseconds(10);
+
+struct Request {
+    uint64_t p = 0, iters = 0;
+    int engine = 0;
+    bool want_words = false;
+    llg_result res{};
+    std::vector<uint64_t> words;
+    int rc = LLG_OK;
+    std::string err;
+    bool done = false, lead = false;
+};
+
+struct CallPool {
+    std::mutex mx;
+    std::condition_variable cv;
+    std::vector<Request*> pending;
+    bool leading = false;
+    size_t last_round = 1;  // requests in the previous round
+};
+
+std::mutex g_pools_mx;
+std::map<int, std::unique_ptr<CallPool>> g_pools;  // per device ordinal
+
+CallPool& call_pool(int dev) {
+    std::lock_guard<std::mutex> lk(g_pools_mx);
+    std::unique_ptr<CallPool>& p = g_pools[dev];
+    if (!p) p.reset(new CallPool());
+    return *p;
+}
+
+int run_sync(llg_batch* b);
+void destroy_batch(llg_batch* b);
+
+// One round: every request of `reqs`, one batch per engine.
+void run_round(std::vector<Request*>& reqs) {
+    for (int engine : {LLG_ENGINE_FP64, LLG_ENGINE_NTT}) {
+        std::vector<Request*> mine;
+        for (Request* r : reqs)
+            if (r->engine == engine) mine.push_back(r);
+        if (mine.empty()) continue;
+        std::vector<uint64_t> ps, its;
+        bool words = false;
+        for (Request* r : mine) {
+            ps.push_back(r->p);
+            its.push_back(r->iters);
+            words = words || r->want_words;
+        }
+        llg_batch* b = nullptr;
+        int rc = make_batch(ps.data(), ps.size(), 0, engine, 0, false, words ? LLG_BATCH_KEEP_WORDS : 0, &b, its.data());
+        if (!rc) rc = run_sync(b);
+        std::vector<llg_result> out(ps.size());
+        std::vector<uint64_t> wbuf;
+        if (!rc) {
+            size_t total = 0;
+            for (uint64_t p : ps) total += (size_t)((p + 63) / 64);
+            if (words) wbuf.resize(total);
+            rc = llg_batch_results(b, out.data(), words ? wbuf.data() : nullptr, wbuf.size());
+        }
+        if (b) destroy_batch(b);
+        size_t off = 0;
+        for (size_t i = 0; i < mine.size(); ++i) {
+            Request* r = mine[i];
+            const size_t nw = (size_t)((r->p + 63) / 64);
+            r->rc = rc;
+            if (rc) r->err = t_last_error;
+            else r->res = out[i];
+            if (!rc && r->want_words) r->words.assign(wbuf.begin() + off, wbuf.begin() + off + nw);
+            off += nw;
+        }
+    }
+}
+
+// Runs `r` through the device's pool; returns when its result is in.
+void run_pooled(int dev, Request& r) {
+    CallPool& P = call_pool(dev);
+    std::unique_lock<std::mutex> lk(P.mx);
+    P.pending.push_back(&r);
+    if (!P.leading) {
+        P.leading = true;
+        r.lead = true;
+    }
+    P.cv.wait(lk, [&] { return r.done || r.lead; });
+    if (r.done) return;
+    // lead this round
+    const auto window = P.last_round > 1 ? kGatherWindow : kGatherWindowAlone;
+    lk.unlock();
+    std::this_thread::sleep_for(window);
+    lk.lock();
+    std::vector<Request*> round;
+    round.swap(P.pending);
+    P.last_round = round.size();
+    lk.unlock();
+    run_round(round);
+    lk.lock();
+    for (Request* q : round) q->done = true;
+    if (!P.pending.empty()) P.pending.front()->lead = true;
+    else P.leading = false;
+    P.cv.notify_all();
+}
+
 }  // namespace
 
 namespace llg {
@@ -933,6 +1047,29 @@ int llg_run(uint64_t p, uint64_t max_iters, int engine, uint32_t n, llg_result* 
     if (!out) return fail(LLG_E_ARG, "null result pointer");
     const size_t nw = (size_t)((p + 63) / 64);
     if (words && nwords < nw) return fail(LLG_E_ARG, "words buffer too small (%zu < %zu)", nwords, nw);
+    if (n == 0 && (engine == LLG_ENGINE_FP64 || engine == LLG_ENGINE_NTT)) {
+        // whole-test lengths (and the word path): share a batch with concurrent callers
+        const uint32_t len = p < kWordMaxP ? 0 : (engine == LLG_ENGINE_NTT ? ntt_len(p) : fp64_length(p, g_max_bpw));
+        if (p < kWordMaxP || (len && is_small_length(len))) {
+            int dev;
+            int rc = device_ready(&dev);
+            if (rc) return rc;
+            Request r;
+            r.p = p;
+            r.iters = max_iters;
+            r.engine = engine;
+            r.want_words = words != nullptr;
+            run_pooled(dev, r);
+            if (r.rc) return fail(r.rc, "%s", r.err.c_str());
+            *out = r.res;
+            if (words) {
+                std::memset(words, 0, nwords * sizeof(uint64_t));
+                std::memcpy(words, r.words.data(), std::min(nw, r.words.size()) * sizeof(uint64_t));
+            }
+            if (out->status) return fail(out->status, "p=%llu: %s", (unsigned long long)p, llg_status_string(out->status));
+            return LLG_OK;
+        }
+    }
     llg_batch* b = nullptr;
     int rc = make_batch(&p, 1, max_iters, engine, n, true, words ? LLG_BATCH_KEEP_WORDS : 0, &b);
     if (rc) return rc;
@@ -1148,6 +1285,8 @@ int llg_test_errlog(llg_test* t, float* log, size_t cap, size_t* len) {
     if (!t->f) return fail(LLG_E_ARG, "the NTT engine has no round-off log (it is exact)");
     const size_t have = (size_t)std::min<uint64_t>(t->f->done, (uint64_t)t->f->errlog_len);
     const size_t n = std::min(cap, have);
+    // the squarings may still run on any stream: wait for the device before reading the log
+    CK(cudaDeviceSynchronize());
     CK(cudaMemcpy(log, t->f->errlog, n * sizeof(float), cudaMemcpyDeviceToHost));
     if (len) *len = n;
     return LLG_OK;

@@ -54,6 +54,35 @@ __device__ __forceinline__ double2 rot(double2 a) {
     return make_double2(fma(a.x, c, a.y * s), fma(a.y, c, -a.x * s));
 }
 
+// rot<16, k16, INV> for a k16 known only after unrolling (the switch folds away).
+template <bool INV>
+__device__ __forceinline__ double2 rot16_k(double2 a, int k16) {
+    switch (k16 & 15) {
+        case 0: return a;
+        case 1: return rot<16, 1, INV>(a);
+        case 2: return rot<16, 2, INV>(a);
+        case 3: return rot<16, 3, INV>(a);
+        case 4: return rot<16, 4, INV>(a);
+        case 5: return rot<16, 5, INV>(a);
+        case 6: return rot<16, 6, INV>(a);
+        case 7: return rot<16, 7, INV>(a);
+        case 8: return rot<16, 8, INV>(a);
+        case 9: return rot<16, 9, INV>(a);
+        case 10: return rot<16, 10, INV>(a);
+        case 11: return rot<16, 11, INV>(a);
+        case 12: return rot<16, 12, INV>(a);
+        case 13: return rot<16, 13, INV>(a);
+        case 14: return rot<16, 14, INV>(a);
+        default: return rot<16, 15, INV>(a);
+    }
+}
+// Multiply by e^{-2 pi i k / R} (INV: e^{+2 pi i k / R}), R in {1, 2, 4, 8, 16}.
+template <int R, bool INV>
+__device__ __forceinline__ double2 rot_k(double2 a, int k) {
+    if constexpr (R == 1) return a;
+    else return rot16_k<INV>(a, (k & (R - 1)) * (16 / R));
+}
+
 // In-register DFT of R points, natural order in and out:
 //   X_k = sum_n x_n e^{-+2 pi i nk/R}   (sign - for the forward transform, + for INV; unscaled).
 template <int R, bool INV>

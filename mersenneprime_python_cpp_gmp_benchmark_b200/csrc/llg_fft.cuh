@@ -42,6 +42,21 @@ __device__ __forceinline__ int phys(int x) { return x + (x >> 4); }
 template <int PADLOG>
 __device__ __forceinline__ int physp(int x) { return x + (x >> PADLOG); }
 
+// Digit reversal of the first P-1 radix-E digits: freq_of_pos(pos) = freq_rev(pos / RLAST) +
+// (pos % RLAST) * (M / RLAST). For pos = t E + j (RLAST divides E) the first term depends on t and
+// j / RLAST only, and w_M^{(pos % RLAST) M / RLAST} is an RLAST-th root of unity: the real-FFT
+// split's twiddle w_M^freq is one table value per j / RLAST times an exact rotation.
+template <class G>
+__device__ __forceinline__ int freq_rev(int rest) {
+    int k = 0;
+#pragma unroll
+    for (int s = 0; s < G::P - 1; ++s) {
+        k = (k << G::LE) | (rest & (G::E - 1));
+        rest >>= G::LE;
+    }
+    return k;
+}
+
 // Frequency index k of DIF output position pos (mixed radix E,...,E,RLAST digit reversal).
 template <class G>
 __device__ __forceinline__ int freq_of_pos(int pos) {

@@ -30,7 +30,7 @@ struct LargeTest {
     int logN = 0, logC = 0, logR = 0, C = 0, R = 0, rows = 0, nblocks = 0;
     double2* V = nullptr;
     double* carry = nullptr;
-    float* carry2 = nullptr;
+    double* carry2 = nullptr;
     LargeCtl* ctl = nullptr;
     unsigned* flags = nullptr;
     int* digits = nullptr;

@@ -156,7 +156,7 @@ struct LargeArgs {
     const int* sB;            // [C] (-2Rb p) mod N
     double* carry;            // [nblocks + 1][C] hop-1 carry-outs of a tile's last row (integers):
                               // slot 0 the wrap-around job's (row R-1, one column on), k + 1 tile k's
-    float* carry2;            // [nblocks + 1][C] hop-2 carry-outs (integers of a few units)
+    double* carry2;           // [nblocks + 1][C] hop-2 carry-outs (integers of a few units)
     LargeCtl* ctl;
     unsigned int* flags;      // [nblocks + 1] epoch + 1 once the job of that slot published its carries
     unsigned long long spin_limit;  // bound of every wait on a flag (x ~64 ns sleeps)

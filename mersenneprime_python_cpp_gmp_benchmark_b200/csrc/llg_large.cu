@@ -144,45 +144,50 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blo
     } else {
         // ---- the tile's rows, straight into registers: thread (row, tr) holds positions
         //      tr E .. tr E + E-1 (the forward FFT's output order), G rows per 16 G-byte run ----
+        {
+            const double2* lp = A.V + (size_t)(tr * E) * R + a;
 #pragma unroll
-        for (int j = 0; j < E; ++j) v[j] = __ldcg(A.V + (size_t)(tr * E + j) * R + a);
+            for (int j = 0; j < E; ++j) v[j] = __ldcg(lp + (size_t)j * R);
+        }
         // the twiddle table (L2-resident) is fetched while the rows' loads are in flight
         for (int k = t; k < QL; k += T) qtw[k] = A.qtwC[k];
         __syncthreads();
         inverse_from<GC, GC::P - 1, false, CtaSync, G, LE>(v, buf, qtw, tr, sync);
 
         // ---- hop 1: unweight, round, round-off, two-digit chain from zero; hop 2 for rows fed
-        //      from inside the tile (the carry-out of the lane above). Row G-1 publishes its
+        //      from inside the tile (the carry-out of the lane above); hop 3 for rows 2 .. G-1 (the
+        //      hop-2 carry-out of the row above, also known inside the tile). Row G-1 publishes its
         //      hop-1 and hop-2 carry-outs for the next tile (the wrap job: one column on). ----
         const int slot = job + 1;
         const double ia0 = __ldg(A.iwA + 2 * a), ia1 = __ldg(A.iwA + 2 * a + 1);
         double lerr = 0.0;
-        float c2s[E];
 #pragma unroll
         for (int i = 0; i < E; ++i) {
             const int b = tr + TR * i;
             const double iwb = __ldg(A.iwB + b);
             const uint32_t kd = digit_kind(b);
-            const bool w0 = kd & 1u, w1 = kd & 2u;
+            const int w0 = kd & 1u, w1 = (kd >> 1) & 1u;
             const double va = v[i].x * (ia0 * iwb) * ((kd & 4u) ? 2.0 : 1.0);
             const double vb = v[i].y * (ia1 * iwb) * ((kd & 8u) ? 2.0 : 1.0);
             long long ia, ib;
             const double r0 = round_shift(va, ia), r1 = round_shift(vb, ib);
             lerr = fmax(lerr, fmax(fabs(va - r0), fabs(vb - r1)));
-            double c, c1;
+            double c, c1, c2 = 0.0;
             double x0 = dsplit_e(r0, A.q + w0, c);
             double x1 = dsplit_e(r1 + c, A.q + w1, c1);
-            const int col = wrap_job ? ((b + 1) & (C - 1)) : b;  // row R-1, column b feeds row 0, column b+1
-            if (ra == G - 1) A.carry[(size_t)slot * C + col] = c1;
             const double cin = __shfl_up_sync(FULL, c1, 1, G);
-            double c2 = 0.0;
             if (ra > 0) {
                 x0 = dsplit_e(x0 + cin, A.q + w0, c);
                 x1 = dsplit_e(x1 + c, A.q + w1, c2);
             }
-            if (ra == G - 1) A.carry2[(size_t)slot * C + col] = (float)c2;
+            const double cin2 = __shfl_up_sync(FULL, c2, 1, G);
+            if (ra > 1) x0 += cin2;
+            if (ra == G - 1) {
+                const int col = wrap_job ? ((b + 1) & (C - 1)) : b;  // row R-1, column b feeds row 0, column b+1
+                A.carry[(size_t)slot * C + col] = c1;
+                A.carry2[(size_t)slot * C + col] = c2;
+            }
             v[i] = make_double2(x0, x1);
-            c2s[i] = (float)c2;
         }
         // the tile's round-off max: one shared atomic per warp
 #pragma unroll
@@ -202,27 +207,27 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blo
             }
         }
         if (wrap_job) return;
-        // ---- the tile's first row: hops 2 and 3 from the previous tile's last row (or the wrap) ----
+        // ---- the tile's first row: hops 2 and 3 from the previous tile's last row (or the wrap);
+        //      its hop-2 carry-out is hop 3 of the second row ----
         if (t == 0) wait_flag(&A.flags[job], ep + 1u, A.ctl, A.spin_limit);
         __syncthreads();
-        // (written without a branch on the row: every lane computes, the first row's lanes keep it)
-        const bool first = ra == 0;
         const double* cprev = A.carry + (size_t)job * C;
-        const float* c2prev = A.carry2 + (size_t)job * C;
+        const double* c2prev = A.carry2 + (size_t)job * C;
 #pragma unroll
         for (int i = 0; i < E; ++i) {
             const int b = tr + TR * i;
-            const uint32_t kd = digit_kind(b);
-            const bool w0 = kd & 1u, w1 = kd & 2u;
-            double cin = first ? __ldcg(cprev + b) : 0.0;
-            if (a == 0 && b == 0) cin -= 2.0;  // the "- 2" of s^2 - 2 (digit 0)
-            const float cin2 = first ? __ldcg(c2prev + b) : 0.f;
-            double c, c2;
-            const double x0 = dsplit_e(v[i].x + cin, A.q + w0, c);
-            const double x1 = dsplit_e(v[i].y + c, A.q + w1, c2);
-            // ---- hop 3: the hop-2 carry-out of the row above (the previous tile's for row 0) ----
-            const float up = __shfl_up_sync(FULL, first ? (float)c2 : c2s[i], 1, G);
-            v[i] = first ? make_double2(x0 + (double)cin2, x1) : make_double2(v[i].x + (double)up, v[i].y);
+            double c2 = 0.0;
+            if (ra == 0) {
+                const uint32_t kd = digit_kind(b);
+                double cin = __ldcg(cprev + b);
+                if (a == 0 && b == 0) cin -= 2.0;  // the "- 2" of s^2 - 2 (digit 0)
+                double c;
+                const double x0 = dsplit_e(v[i].x + cin, A.q + (int)(kd & 1u), c);
+                const double x1 = dsplit_e(v[i].y + c, A.q + (int)((kd >> 1) & 1u), c2);
+                v[i] = make_double2(x0 + __ldcg(c2prev + b), x1);
+            }
+            const double up = __shfl_up_sync(FULL, c2, 1, G);
+            if (ra == 1) v[i].x += up;
         }
         if (MODE == LARGE_FINAL || A.dump) {
 #pragma unroll
@@ -249,8 +254,12 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blo
         if (t == 0) wait_flag(&A.flags[0], ep + 1u, A.ctl, A.spin_limit);
         __syncthreads();
     }
+    // the store addresses equal the load addresses; formed again here from an opaque base, so the
+    // compiler does not keep sixteen 64-bit addresses live across the whole pass
+    double2* vp = A.V + (size_t)(tr * E) * R + a;
+    asm volatile("" : "+l"(vp));
 #pragma unroll
-    for (int j = 0; j < E; ++j) __stcg(A.V + (size_t)(tr * E + j) * R + a, v[j]);
+    for (int j = 0; j < E; ++j) __stcg(vp + (size_t)j * R, v[j]);
 }
 
 // Column pass: one block owns the column pair (c, C-c), one half of its threads per column; the
@@ -294,7 +303,13 @@ __global__ void __launch_bounds__(2 * (1 << LOG_R) / (1 << kLargeLogE), (LOG_R <
 #pragma unroll
     for (int j = 0; j < E; ++j) buf[phys(tc * E + j)] = v[j];
     __syncthreads();
+    // w_M^{c + C d} for the column frequency d of position tc E + j: w_M^c times one table value
+    // w_R^{freq_rev} per j / RLAST, times the exact rotation w_RLAST^(j % RLAST)
     const double2 wc = __ldg(A.tw1 + c);  // w_M^c
+    constexpr int RL = GR::RLAST, NB = E / RL;
+    double2 wk[NB];
+#pragma unroll
+    for (int h = 0; h < NB; ++h) wk[h] = cmul(wc, twiddle<LOG_R>(qtw, (uint32_t)freq_rev<GR>(tc * NB + h), false));
 #pragma unroll
     for (int j = 0; j < E; ++j) {
         const int d = freq_of_pos<GR>(tc * E + j);
@@ -304,8 +319,7 @@ __global__ void __launch_bounds__(2 * (1 << LOG_R) / (1 << kLargeLogE), (LOG_R <
         const double2 s = cadd(Av, Bc), dd = csub(Av, Bc);
         const double2 a3 = make_double2(3.0 * Av.x - Bc.x, 3.0 * Av.y - Bc.y);
         const double2 d2 = make_double2((dd.x - dd.y) * (dd.x + dd.y), 2.0 * dd.x * dd.y);
-        const double2 w = cmul(wc, twiddle<LOG_R>(qtw, (uint32_t)d, false));  // w_M^{c + C d}
-        v[j] = csub(cmul(a3, s), cmul(w, d2));
+        v[j] = csub(cmul(a3, s), cmul(wk[j / RL], rot_k<RL, false>(d2, j % RL)));
     }
     __syncthreads();  // partner reads done before either column overwrites its buffer
     inverse_from<GR, GR::P - 1, false>(v, buf, qtw, tc, gsync);
@@ -329,10 +343,23 @@ static size_t col_smem() {
     return sizeof(double2) * 2 * GR::PAD + sizeof(double2) * qpad_len(GR::M / 4) + sizeof(double2) * 2 * GR::E;
 }
 
+// Shared-memory carve-out (percent of the SM's 228 KB) for `blocks` resident blocks of `bytes`
+// dynamic shared memory each: no more than they need, so the rest of the on-chip memory stays L1
+// (register spills and the weight-table reads hit there).
+static int carveout_pct(size_t bytes, int blocks) {
+    const size_t need = (size_t)blocks * (bytes + 1024 + 64);  // + the per-block reservation and statics
+    const int pct = (int)((100 * need + 228 * 1024 - 1) / (228 * 1024));
+    return pct > 100 ? 100 : pct;
+}
+
 template <int LOG_C, int G, int MODE>
 static cudaError_t row_attr() {
-    return cudaFuncSetAttribute(large_row<LOG_C, G, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)row_smem<LOG_C, G>());
+    cudaError_t e = cudaFuncSetAttribute(large_row<LOG_C, G, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)row_smem<LOG_C, G>());
+    if (!e)
+        e = cudaFuncSetAttribute(large_row<LOG_C, G, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 carveout_pct(row_smem<LOG_C, G>(), large_row_min_blocks(LOG_C, G)));
+    return e;
 }
 
 template <int LOG_C, int G>
@@ -345,8 +372,12 @@ static cudaError_t row_attrs() {
 
 template <int LOG_R>
 static cudaError_t col_attr() {
-    return cudaFuncSetAttribute(large_col<LOG_R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)col_smem<LOG_R>());
+    cudaError_t e = cudaFuncSetAttribute(large_col<LOG_R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)col_smem<LOG_R>());
+    if (!e)
+        e = cudaFuncSetAttribute(large_col<LOG_R>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 carveout_pct(col_smem<LOG_R>(), LOG_R <= 11 ? 2 : 1));
+    return e;
 }
 
 // INIT: one block per tile. ITER / FINAL: one block more, for the wrap-around job (grid == 0), or

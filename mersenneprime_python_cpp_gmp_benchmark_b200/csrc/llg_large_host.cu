@@ -167,7 +167,7 @@ cudaError_t LargeTest::init(uint64_t p_, int log_n, int log_c, int rows_) {
     if ((e = cudaMalloc(&V, M * sizeof(double2)))) return e;
     // carry slots and flags: one per tile plus slot 0 for the wrap-around job
     if ((e = cudaMalloc(&carry, (size_t)(nblocks + 1) * C * sizeof(double)))) return e;
-    if ((e = cudaMalloc(&carry2, (size_t)(nblocks + 1) * C * sizeof(float)))) return e;
+    if ((e = cudaMalloc(&carry2, (size_t)(nblocks + 1) * C * sizeof(double)))) return e;
     if ((e = cudaMalloc(&ctl, sizeof(LargeCtl)))) return e;
     if ((e = cudaMemset(ctl, 0, sizeof(LargeCtl)))) return e;
     if ((e = cudaMalloc(&flags, (size_t)(nblocks + 1) * sizeof(unsigned)))) return e;

@@ -77,7 +77,7 @@ Layout layout(int logN, int logC, int logR, int s) {
     size_t o = 0;
     L.V = o; o = up256(o + M * sizeof(double2));
     L.carry = o; o = up256(o + (nblocks + 1) * C * sizeof(double));  // slot 0: the wrap-around job
-    L.carry2 = o; o = up256(o + (nblocks + 1) * C * sizeof(float));
+    L.carry2 = o; o = up256(o + (nblocks + 1) * C * sizeof(double));
     L.ctl = o; o = up256(o + sizeof(LargeCtl));
     L.flags = o; o = up256(o + (nblocks + 1) * sizeof(unsigned));
     L.qtwC = o; o = up256(o + qpad_len((uint32_t)C) * sizeof(double2));
@@ -221,7 +221,7 @@ extern "C" int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* 
     A.iwB = reinterpret_cast<const double*>(base + L.iwB);
     A.sB = reinterpret_cast<const int*>(base + L.sB);
     A.carry = reinterpret_cast<double*>(base + L.carry);
-    A.carry2 = reinterpret_cast<float*>(base + L.carry2);
+    A.carry2 = reinterpret_cast<double*>(base + L.carry2);
     A.ctl = reinterpret_cast<LargeCtl*>(base + L.ctl);
     A.flags = reinterpret_cast<unsigned*>(base + L.flags);
     A.digits = digits_out;

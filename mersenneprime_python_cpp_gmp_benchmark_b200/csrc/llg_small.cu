@@ -125,6 +125,11 @@ __global__ void __launch_bounds__(SmallGeo<LOG_M>::T, small_min_blocks(SmallGeo<
         }
         __syncthreads();
         if (active) {
+            // w^k of position t E + j: one table value per j / RLAST, times w_RLAST^(j % RLAST)
+            constexpr int RL = G::RLAST, NB = E / RL;
+            double2 wk[NB];
+#pragma unroll
+            for (int h = 0; h < NB; ++h) wk[h] = twiddle_g<G>(qtw, (uint32_t)freq_rev<G>(t * NB + h), false);
 #pragma unroll
             for (int j = 0; j < E; ++j) {
                 const int k = freq_of_pos<G>(t * E + j);
@@ -134,8 +139,7 @@ __global__ void __launch_bounds__(SmallGeo<LOG_M>::T, small_min_blocks(SmallGeo<
                 const double2 s = cadd(A, Bc), d = csub(A, Bc);
                 const double2 a3 = make_double2(3.0 * A.x - Bc.x, 3.0 * A.y - Bc.y);
                 const double2 d2 = make_double2((d.x - d.y) * (d.x + d.y), 2.0 * d.x * d.y);
-                const double2 w = twiddle_g<G>(qtw, (uint32_t)k, false);
-                v[j] = csub(cmul(a3, s), cmul(w, d2));
+                v[j] = csub(cmul(a3, s), cmul(wk[j / RL], rot_k<RL, false>(d2, j % RL)));
             }
             // the first inverse pass stores only after a barrier (partners may still be reading)
             inverse_from<G, G::P - 1>(v, buf, qtw, t);

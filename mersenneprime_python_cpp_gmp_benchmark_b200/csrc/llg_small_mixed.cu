@@ -178,6 +178,13 @@ __global__ void __launch_bounds__(MixedGeom<R0, LOG_L>::T, mixed_min_blocks(Mixe
         __syncthreads();
         {
             const int segp = (seg == 0) ? 0 : R0 - seg;
+            // w_M^{R0 kk + seg} with kk = freq_rev(tl NB + j / RL) + (j % RL) L / RL: one table
+            // value per j / RL, times the exact rotation w_RL^(j % RL)
+            constexpr int RL = GL::RLAST, NB = E / RL;
+            double2 wk[NB];
+#pragma unroll
+            for (int h = 0; h < NB; ++h)
+                wk[h] = twiddle_m<M>(qtwM, (uint32_t)(R0 * freq_rev<GL>(tl * NB + h) + seg), false);
 #pragma unroll
             for (int j = 0; j < E; ++j) {
                 const int kk = freq_of_pos<GL>(tl * E + j);
@@ -187,8 +194,7 @@ __global__ void __launch_bounds__(MixedGeom<R0, LOG_L>::T, mixed_min_blocks(Mixe
                 const double2 s = cadd(A, Bc), d = csub(A, Bc);
                 const double2 a3 = make_double2(3.0 * A.x - Bc.x, 3.0 * A.y - Bc.y);
                 const double2 d2 = make_double2((d.x - d.y) * (d.x + d.y), 2.0 * d.x * d.y);
-                const double2 w = twiddle_m<M>(qtwM, (uint32_t)(R0 * kk + seg), false);
-                v[j] = csub(cmul(a3, s), cmul(w, d2));
+                v[j] = csub(cmul(a3, s), cmul(wk[j / RL], rot_k<RL, false>(d2, j % RL)));
             }
         }
         __syncthreads();  // partner reads (other segments) done before any segment stores

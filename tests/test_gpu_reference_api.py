@@ -106,3 +106,35 @@ sys.exit(0 if hits == known and sorted(cuda_hits) == known else 2)
 '''
     r = subprocess.run([sys.executable, "-c", code, PKG], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
+
+
+def test_concurrent_callers_share_batches(gpu, oracle):
+    """Single-exponent calls from many host threads at once (the driver's thread pool) are pooled
+    into shared batches: every caller gets its own exact result, whether it asked for a full test or
+    an interim residue, for its words or not, on either engine."""
+    from concurrent.futures import ThreadPoolExecutor
+    from conftest import load_range
+    gold = load_range()
+    ps = [p for p in range(3, 6000) if p in gold]
+    jobs = []
+    for i, p in enumerate(ps):
+        if i % 7 == 3:
+            jobs.append((p, 0, "ntt", False))
+        elif i % 11 == 5 and p > 300:
+            jobs.append((p, 50, "fp64", True))
+        else:
+            jobs.append((p, 0, "fp64", False))
+
+    def one(job):
+        p, k, engine, words = job
+        return job, gpu.run(p, iters=k, engine=engine, want_words=words)
+
+    with ThreadPoolExecutor(32) as ex:
+        results = list(ex.map(one, jobs))
+    for (p, k, engine, words), r in results:
+        assert r["status"] == 0, (p, engine)
+        if k == 0:
+            assert (bool(r["is_zero"]), r["res64"]) == gold[p][:2], (p, engine)
+        else:
+            want = oracle.ll_gmp(p, k)
+            assert r["res64"] == want[1] and r["words"] == want[2], p
