@@ -86,6 +86,8 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blo
     constexpr int QL = (int)twiddle_table_len<GC>();
     double2* xbuf = reinterpret_cast<double2*>(smem_raw);          // exchange: slot physp(x) * G + row
     double2* qtw = xbuf + large_row_slots(LOG_C, G);               // padded twiddle table (C-point)
+    double* swB = reinterpret_cast<double*>(qtw + QL);             // C column weights 2^(sB/N)
+    double* siwB = swB + C;                                        // C inverse column weights
     __shared__ unsigned long long s_err;
     __shared__ int s_job;
     __shared__ unsigned s_epoch;
@@ -140,6 +142,7 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blo
             v[i] = make_double2((double)d.x, (double)d.y);
         }
         for (int k = t; k < QL; k += T) qtw[k] = A.qtwC[k];
+        for (int k = t; k < C; k += T) swB[k] = __ldg(A.wB + k);
         __syncthreads();
     } else {
         // ---- the tile's rows, straight into registers: thread (row, tr) holds positions
@@ -149,8 +152,13 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blo
 #pragma unroll
             for (int j = 0; j < E; ++j) v[j] = __ldcg(lp + (size_t)j * R);
         }
-        // the twiddle table (L2-resident) is fetched while the rows' loads are in flight
+        // the twiddle and column-weight tables (L2-resident) are fetched while the rows' loads are
+        // in flight
         for (int k = t; k < QL; k += T) qtw[k] = A.qtwC[k];
+        for (int k = t; k < C; k += T) {
+            swB[k] = __ldg(A.wB + k);
+            siwB[k] = __ldg(A.iwB + k);
+        }
         __syncthreads();
         inverse_from<GC, GC::P - 1, false, CtaSync, G, LE>(v, buf, qtw, tr, sync);
 
@@ -164,7 +172,7 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blo
 #pragma unroll
         for (int i = 0; i < E; ++i) {
             const int b = tr + TR * i;
-            const double iwb = __ldg(A.iwB + b);
+            const double iwb = siwB[b];
             const uint32_t kd = digit_kind(b);
             const int w0 = kd & 1u, w1 = (kd >> 1) & 1u;
             const double va = v[i].x * (ia0 * iwb) * ((kd & 4u) ? 2.0 : 1.0);
@@ -243,7 +251,7 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blo
     const double wa0 = __ldg(A.wA + 2 * a), wa1 = __ldg(A.wA + 2 * a + 1);
 #pragma unroll
     for (int i = 0; i < E; ++i) {
-        const double wb = __ldg(A.wB + tr + TR * i);
+        const double wb = swB[tr + TR * i];
         const uint32_t kd = digit_kind(tr + TR * i);
         v[i].x *= (wa0 * wb) * ((kd & 4u) ? 0.5 : 1.0);
         v[i].y *= (wa1 * wb) * ((kd & 8u) ? 0.5 : 1.0);
@@ -267,12 +275,14 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blo
 // Block 0 holds column 0 and block C/2 column C/2, each of which pairs with itself.
 template <int LOG_R>
 __global__ void __launch_bounds__(2 * (1 << LOG_R) / (1 << kLargeLogE), (LOG_R <= 11 ? 2 : 1)) large_col(const LargeArgs A) {
-    using GR = SmallG<LOG_R, kLargeLogE>;
+    // quarter twiddle table in the spread layout (entry r at qpad_s(r)): the strided twiddle reads
+    // of the radix passes spread over more bank groups than with qpad
+    using GR = SmallG<LOG_R, kLargeLogE, TW_QUARTER_S>;
     constexpr int R = GR::M, TC = GR::T, E = GR::E;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2* bufs = reinterpret_cast<double2*>(smem_raw);  // 2 exchange buffers of PAD slots
     double2* qtw = bufs + 2 * GR::PAD;                       // padded quarter table (R-point)
-    constexpr int QL = (int)qpad_len(R / 4);
+    constexpr int QL = (int)qpad_s_len(R / 4);
     const int t = threadIdx.x, half = t / TC, tc = t % TC;
     const int C = A.C;
     const int cb = blockIdx.x;  // 0 .. C/2
@@ -309,7 +319,7 @@ __global__ void __launch_bounds__(2 * (1 << LOG_R) / (1 << kLargeLogE), (LOG_R <
     constexpr int RL = GR::RLAST, NB = E / RL;
     double2 wk[NB];
 #pragma unroll
-    for (int h = 0; h < NB; ++h) wk[h] = cmul(wc, twiddle<LOG_R>(qtw, (uint32_t)freq_rev<GR>(tc * NB + h), false));
+    for (int h = 0; h < NB; ++h) wk[h] = cmul(wc, twiddle<LOG_R, true>(qtw, (uint32_t)freq_rev<GR>(tc * NB + h), false));
 #pragma unroll
     for (int j = 0; j < E; ++j) {
         const int d = freq_of_pos<GR>(tc * E + j);
@@ -331,16 +341,170 @@ __global__ void __launch_bounds__(2 * (1 << LOG_R) / (1 << kLargeLogE), (LOG_R <
     if (cb == 0 && t == 0) atomicAdd(&A.ctl->epoch, 1u);
 }
 
+// e^{-2 pi i x / R} (conjugated when inv) for x < R, R a multiple of 4, from the padded quarter
+// table of R points (R need not be a power of two).
+template <int R>
+__device__ __forceinline__ double2 twiddle_r(const double2* __restrict__ q, uint32_t x, bool inv) {
+    constexpr uint32_t QR = (uint32_t)R / 4;
+    const uint32_t quad = x / QR;
+    const double2 w = q[qpad(x - quad * QR)];
+    double2 r;
+    switch (quad & 3u) {
+        case 0: r = w; break;
+        case 1: r = make_double2(w.y, -w.x); break;
+        case 2: r = make_double2(-w.x, -w.y); break;
+        default: r = make_double2(-w.y, w.x); break;
+    }
+    return inv ? conj2(r) : r;
+}
+
+// acc + a w + b conj(w): the radix-R0 terms of r and R0 - r share their factor up to conjugation.
+__device__ __forceinline__ double2 pair_term_r(double2 acc, double2 a, double2 b, double2 w) {
+    const double sx = a.x + b.x, sy = a.y + b.y, dx = a.x - b.x, dy = a.y - b.y;
+    return make_double2(fma(-dy, w.y, fma(sx, w.x, acc.x)), fma(dx, w.y, fma(sy, w.x, acc.y)));
+}
+
+// Column pass at the non-power-of-two column lengths R = R0 L (R0 = 3 or 5, L = 2^LOG_L, 16 values
+// per thread), for the {3, 5} x 2^k transform lengths of the reference (lucaslehmer.cpp:244-254).
+// One block owns the column pair (c, C-c) as in large_col; each column is split as R0 x L by
+// decimation in frequency (a = n + L r, d = R0 k' + k0):
+//   U[R0 k' + k0] = sum_n w_L^{n k'} w_R^{n k0} sum_r u[n + L r] w_R0^{r k0}
+// the radix-R0 step across the column's R0 segments, the twiddle w_R^{n k0}, R0 L-point FFTs
+// (one segment of L/16 threads each, a named barrier per segment), the real-FFT split and square
+// over the pair, and back. Thread (half, seg, tl) holds u[seg L + tl + TL i] of its column.
+template <int R0, int LOG_L>
+__global__ void __launch_bounds__(2 * R0 * (1 << LOG_L) / (1 << kLargeLogE), (2 * R0 * (1 << LOG_L) / (1 << kLargeLogE) <= 256 ? 2 : 1))
+    large_col_mixed(const LargeArgs A) {
+    using GL = SmallG<LOG_L, kLargeLogE>;
+    constexpr int L = GL::M, TL = GL::T, E = GL::E, R = R0 * L, TC = R0 * TL, PADL = GL::PAD;
+    constexpr int QLL = (int)qpad_len(L / 4), QLR = (int)qpad_len(R / 4);
+    static_assert(TL % 32 == 0 && 2 * TC <= 1024, "whole warps per segment");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* bufs = reinterpret_cast<double2*>(smem_raw);  // [half][seg] exchange buffers of PADL slots
+    double2* qtwL = bufs + 2 * R0 * PADL;                    // L-point quarter table
+    double2* qtwR = qtwL + QLL;                              // R-point quarter table
+    double2* omf = qtwR + QLR;                               // [k0][r] w_R0^{r k0}
+    double2* omi = omf + R0 * R0;                            // [r][k0] w_R0^{-r k0}
+    double2* ptabs = omi + R0 * R0;                          // [half][E] w_M^{c TL i}
+    const int t = threadIdx.x, half = t / TC, th = t % TC, seg = th / TL, tl = th % TL;
+    const int C = A.C;
+    const int cb = blockIdx.x;  // 0 .. C/2
+    const int c1 = cb, c2 = (C - cb) & (C - 1);
+    const bool self = (c1 == c2);
+    const bool active = !(self && half == 1);
+    const int c = half ? c2 : c1;
+    double2* hb = bufs + half * R0 * PADL;                  // this column's R0 segment buffers
+    double2* mybuf = hb + seg * PADL;
+    const double2* pb = self ? hb : bufs + (1 - half) * R0 * PADL;  // the partner column's buffers
+    // barriers: 1 + half for the column's threads, 3 + half R0 + seg for one segment's
+    const NamedSync hsync{1u + (unsigned)half, (unsigned)TC};
+    const NamedSync ssync{3u + (unsigned)(half * R0 + seg), (unsigned)TL};
+    for (int k = t; k < QLL; k += 2 * TC) qtwL[k] = A.qtwL[k];
+    for (int k = t; k < QLR; k += 2 * TC) qtwR[k] = A.qtwR[k];
+    if (t < R0 * R0) {
+        // w_R0^{e}, e = (r k0) mod R0, from the R-point table (R / R0 = L)
+        const int x = t / R0, y = t % R0;
+        const uint32_t e = (uint32_t)((x * y) % R0) * (uint32_t)L;
+        omf[t] = twiddle_r<R>(A.qtwR, e, false);  // [k0 = x][r = y]
+        omi[t] = twiddle_r<R>(A.qtwR, e, true);   // [r = x][k0 = y]
+    }
+    double2* col = A.V + (size_t)__ldg(A.pos_of_c + c) * R;
+    // four-step twiddle w_M^{a c}, a = seg L + tl + TL i: w_M^{c (seg L + tl)} w_M^{c TL i}
+    double2* ptab = ptabs + half * E;
+    for (int i = th; i < E; i += TC) ptab[i] = twiddle_M(A, (uint32_t)c * (uint32_t)(TL * i), false);
+    const uint32_t a0 = (uint32_t)(seg * L + tl);
+    const double2 q = twiddle_M(A, (uint32_t)c * a0, false);
+    double2 v[E];
+#pragma unroll
+    for (int i = 0; i < E; ++i) v[i] = active ? col[a0 + TL * i] : make_double2(0.0, 0.0);
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < E; ++i) v[i] = cmul(v[i], cmul(q, ptab[i]));
+    // ---- radix-R0 step across the column's segments, then the twiddle w_R^{n k0} (k0 = seg) ----
+#pragma unroll
+    for (int i = 0; i < E; ++i) mybuf[phys(tl + TL * i)] = v[i];
+    hsync();
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+        const int n = tl + TL * i;
+        double2 acc = hb[phys(n)];
+#pragma unroll
+        for (int r = 1; 2 * r < R0; ++r) acc = pair_term_r(acc, hb[r * PADL + phys(n)], hb[(R0 - r) * PADL + phys(n)], omf[seg * R0 + r]);
+        v[i] = cmul(acc, twiddle_r<R>(qtwR, (uint32_t)(n * seg), false));
+    }
+    hsync();  // every segment read before the L-point FFTs overwrite the buffers
+    forward_from<GL, 0>(v, mybuf, qtwL, tl, ssync);
+#pragma unroll
+    for (int j = 0; j < E; ++j) mybuf[phys(tl * E + j)] = v[j];
+    __syncthreads();
+    // ---- real-FFT split + square over the pair: frequency d = R0 kk + k0 of this column pairs with
+    //      R - 1 - d of column C - c (c == 0: (R - d) mod R of itself) ----
+    {
+        const double2 wc = __ldg(A.tw1 + c);  // w_M^c
+        constexpr int RL = GL::RLAST, NB = E / RL;
+        // w_M^{c + C d} = w_M^c w_R^{k0} w_L^{kk}: one table value per j / RL, times w_RL^(j % RL)
+        const double2 wck = cmul(wc, twiddle_r<R>(qtwR, (uint32_t)seg, false));
+        double2 wk[NB];
+#pragma unroll
+        for (int h = 0; h < NB; ++h) wk[h] = cmul(wck, twiddle<LOG_L>(qtwL, (uint32_t)freq_rev<GL>(tl * NB + h), false));
+#pragma unroll
+        for (int j = 0; j < E; ++j) {
+            const int kk = freq_of_pos<GL>(tl * E + j);
+            int kp, sp;
+            if (c == 0) {
+                const int d = R0 * kk + seg;
+                const int dp = d == 0 ? 0 : R - d;
+                kp = dp / R0;
+                sp = dp - R0 * kp;
+            } else {
+                kp = L - 1 - kk;
+                sp = R0 - 1 - seg;
+            }
+            const int x = sp * PADL + phys(pos_of_freq<GL>(kp));
+            const double2 Av = v[j], Bc = conj2(pb[x]);  // conj(U_{M-k})
+            const double2 sm = cadd(Av, Bc), dd = csub(Av, Bc);
+            const double2 a3 = make_double2(3.0 * Av.x - Bc.x, 3.0 * Av.y - Bc.y);
+            const double2 d2 = make_double2((dd.x - dd.y) * (dd.x + dd.y), 2.0 * dd.x * dd.y);
+            v[j] = csub(cmul(a3, sm), cmul(wk[j / RL], rot_k<RL, false>(d2, j % RL)));
+        }
+    }
+    __syncthreads();  // partner reads done before either column overwrites its buffers
+    inverse_from<GL, GL::P - 1, false>(v, mybuf, qtwL, tl, ssync);
+    // ---- conjugate twiddle and the inverse radix-R0 step: thread (r = seg, tl) gets
+    //      u[n + L r] = sum_k0 w_R0^{-r k0} w_R^{-n k0} z[k0][n] ----
+#pragma unroll
+    for (int i = 0; i < E; ++i) v[i] = cmul(v[i], twiddle_r<R>(qtwR, (uint32_t)((tl + TL * i) * seg), true));
+    ssync();  // this segment's last inverse pass read its buffer
+#pragma unroll
+    for (int i = 0; i < E; ++i) mybuf[phys(tl + TL * i)] = v[i];
+    hsync();
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+        const int n = tl + TL * i;
+        double2 acc = hb[phys(n)];
+#pragma unroll
+        for (int k0 = 1; 2 * k0 < R0; ++k0)
+            acc = pair_term_r(acc, hb[k0 * PADL + phys(n)], hb[(R0 - k0) * PADL + phys(n)], omi[seg * R0 + k0]);
+        v[i] = acc;
+    }
+    if (active) {
+        const double2 q2 = twiddle_M(A, (uint32_t)c * a0, false);  // recomputed: frees registers
+#pragma unroll
+        for (int i = 0; i < E; ++i) col[a0 + TL * i] = cmulc(v[i], cmul(q2, ptab[i]));
+    }
+    if (cb == 0 && t == 0) atomicAdd(&A.ctl->epoch, 1u);
+}
+
 template <int LOG_C, int G>
 static size_t row_smem() {
     using GC = SmallG<LOG_C, large_row_log_e(LOG_C, G), TW_FULL>;
-    return sizeof(double2) * (large_row_slots(LOG_C, G) + twiddle_table_len<GC>());
+    return sizeof(double2) * (large_row_slots(LOG_C, G) + twiddle_table_len<GC>()) + 2 * sizeof(double) * GC::M;
 }
 
 template <int LOG_R>
 static size_t col_smem() {
     using GR = SmallGeom<LOG_R, kLargeLogE>;
-    return sizeof(double2) * 2 * GR::PAD + sizeof(double2) * qpad_len(GR::M / 4) + sizeof(double2) * 2 * GR::E;
+    return sizeof(double2) * 2 * GR::PAD + sizeof(double2) * qpad_s_len(GR::M / 4) + sizeof(double2) * 2 * GR::E;
 }
 
 // Shared-memory carve-out (percent of the SM's 228 KB) for `blocks` resident blocks of `bytes`

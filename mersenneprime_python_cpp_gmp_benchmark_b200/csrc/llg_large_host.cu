@@ -136,7 +136,7 @@ cudaError_t LargeTest::init(uint64_t p_, int log_n, int log_c, int rows_) {
     if ((e = configure_large(logC, rows, logR))) return e;
     // tables
     if ((e = upload(&qtwC, padded_full_table(C)))) return e;
-    if ((e = upload(&qtwR, padded_quarter_table(R)))) return e;
+    if ((e = upload(&qtwR, spread_quarter_table(R)))) return e;  // the column pass reads qpad_s
     if ((e = upload(&tw1, omega_table(M, 1ull << s, 1)))) return e;
     if ((e = upload(&tw2, omega_table(M, M >> s, 1ull << s)))) return e;
     std::vector<int> pc(C);

@@ -42,7 +42,7 @@ namespace llg {
 
 namespace {
 
-constexpr size_t kNoAllocScratchBytes = 640u * 1024u;  // covers N = 65,536 (about 584 KiB used)
+constexpr size_t kNoAllocScratchBytes = 640u * 1024u;  // covers N = 65,536 (about 603 KiB used)
 constexpr int kNoAllocMaxLog = 16;
 constexpr int kMaxDevices = 64;
 
@@ -70,9 +70,12 @@ struct Layout {
 
 size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Rows per row-pass tile: 8 (the fewest tiles, so the fewest carry slots in the array).
+constexpr int kTileRows = 8;
+
 Layout layout(int logN, int logC, int logR, int s) {
     const size_t M = (size_t)1 << (logN - 1), C = (size_t)1 << logC, R = (size_t)1 << logR;
-    const size_t nblocks = R / large_rows_per_block(logC);
+    const size_t nblocks = R / kTileRows;
     Layout L;
     size_t o = 0;
     L.V = o; o = up256(o + M * sizeof(double2));
@@ -81,7 +84,7 @@ Layout layout(int logN, int logC, int logR, int s) {
     L.ctl = o; o = up256(o + sizeof(LargeCtl));
     L.flags = o; o = up256(o + (nblocks + 1) * sizeof(unsigned));
     L.qtwC = o; o = up256(o + qpad_len((uint32_t)C) * sizeof(double2));
-    L.qtwR = o; o = up256(o + qpad_len((uint32_t)(R / 4)) * sizeof(double2));
+    L.qtwR = o; o = up256(o + qpad_s_len((uint32_t)(R / 4)) * sizeof(double2));  // spread layout
     L.tw1 = o; o = up256(o + ((size_t)1 << s) * sizeof(double2));
     L.tw2 = o; o = up256(o + (M >> s) * sizeof(double2));
     L.pos_of_c = o; o = up256(o + C * sizeof(int));
@@ -98,7 +101,7 @@ Layout layout(int logN, int logC, int logR, int s) {
 int pos_of_freq_host(int log_l, int k) {
     // digit reversal of the row FFT's output positions (radix 2^LE passes, the last one RLAST):
     // host copy of pos_of_freq for SmallGeom<log_l, LE>, LE as the row kernel is built
-    const int LE = large_row_log_e(log_l, large_rows_per_block(log_l)), E = 1 << LE;
+    const int LE = large_row_log_e(log_l, kTileRows), E = 1 << LE;
     const int L = 1 << log_l, P = (log_l + LE - 1) / LE;
     const int RLAST = (log_l % LE == 0) ? E : (1 << (log_l % LE));
     const int klast = k / (L / RLAST);
@@ -172,7 +175,7 @@ extern "C" int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* 
     }
     unsigned char* base = g_scratch_addr[dev];
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    e = configure_large(logC, large_rows_per_block(logC), logR);
+    e = configure_large(logC, kTileRows, logR);
     if (e != cudaSuccess) return cuda_fail("configuring the kernels", e);
 
     // tables (exact integers and long-double rounded values, as the allocating path uses), built
@@ -183,7 +186,10 @@ extern "C" int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* 
         const size_t o = L.qtwC;
         std::memset(g_stage, 0, L.end - o);
         stage_table<double2>(L.qtwC - o, qpad_len((uint32_t)C), [&](size_t i) { return padded_quarter_slot(C, i); });
-        stage_table<double2>(L.qtwR - o, qpad_len((uint32_t)R / 4), [&](size_t i) { return padded_quarter_slot(R, i); });
+        {  // the column pass's quarter table in the spread layout: entry r at qpad_s(r)
+            double2* q = reinterpret_cast<double2*>(g_stage + (L.qtwR - o));
+            for (uint32_t r = 0; r < (uint32_t)R / 4; ++r) q[qpad_s(r)] = padded_quarter_slot(R, qpad(r));
+        }
         stage_table<double2>(L.tw1 - o, (size_t)1 << s, [&](size_t i) { return omega(M, i); });
         stage_table<double2>(L.tw2 - o, (size_t)(M >> s), [&](size_t i) { return omega(M, (uint64_t)i << s); });
         stage_table<int>(L.pos_of_c - o, (size_t)C, [&](size_t i) { return pos_of_freq_host(logC, (int)i); });
@@ -232,7 +238,7 @@ extern "C" int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* 
     A.tw_shift = s;
     A.C = C;
     A.R = R;
-    A.nblocks = R / large_rows_per_block(logC);
+    A.nblocks = R / kTileRows;
     A.q = (int)(p >> logN);
     A.rem = (int)(p & (N - 1));
     A.logN = logN;
@@ -251,7 +257,7 @@ extern "C" int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* 
     if ((e = cudaMemsetAsync(A.ctl, 0, sizeof(LargeCtl), st)) != cudaSuccess) return fail_enqueued("clearing the control block", e);
     if ((e = cudaMemsetAsync(A.flags, 0, (size_t)(A.nblocks + 1) * sizeof(unsigned), st)) != cudaSuccess)
         return fail_enqueued("clearing the carry flags", e);
-    const int G = large_rows_per_block(logC);
+    const int G = kTileRows;
     if ((e = launch_large_row(logC, G, LARGE_INIT, A, st)) != cudaSuccess) return fail_enqueued("row pass launch", e);
     if ((e = launch_large_col(logR, A, st)) != cudaSuccess) return fail_enqueued("column pass launch", e);
     for (uint64_t k = 1; k < iters; ++k) {

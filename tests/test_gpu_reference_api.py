@@ -118,7 +118,7 @@ def test_concurrent_callers_share_batches(gpu, oracle):
     ps = [p for p in range(3, 6000) if p in gold]
     jobs = []
     for i, p in enumerate(ps):
-        if i % 7 == 3:
+        if i % 7 == 3 and gpu.ntt_length(p):
             jobs.append((p, 0, "ntt", False))
         elif i % 11 == 5 and p > 300:
             jobs.append((p, 50, "fp64", True))
