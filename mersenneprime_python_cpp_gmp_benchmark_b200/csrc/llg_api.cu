@@ -200,6 +200,9 @@ const std::vector<uint32_t>& fp64_lengths() {
         for (int l = kSmallLogMin; l <= kLargeLogMax; ++l) a.push_back(1u << l);
         for (uint32_t n = 1024; n <= (1u << 14); ++n)
             if (mixed_length_supported(n, nullptr, nullptr)) a.push_back(n);
+        for (uint32_t r = 3; r <= 5; r += 2)
+            for (int k = 18; k <= 21; ++k)
+                if (large_mixed_length_supported((uint64_t)r << k, nullptr, nullptr)) a.push_back(r << k);
         std::sort(a.begin(), a.end());
         return a;
     }();
@@ -208,11 +211,16 @@ const std::vector<uint32_t>& fp64_lengths() {
 
 // The two-pass engine's three-hop carry keeps digits balanced down to ~log2(N)/4 + 1 bits per
 // digit; it asks for floor(p/N) >= log2(N)/4 + 3.
+// Two-pass FP64 lengths: 2^14 .. 2^23 and R0 2^k (large_mixed_length_supported).
+bool large_fp64_length(uint64_t n) {
+    const int l = ilog2_exact(n);
+    return (l > kSmallLogMax && large_length_supported(l)) || large_mixed_length_supported(n, nullptr, nullptr);
+}
+
 bool fp64_length_usable(uint64_t p, uint64_t n) {
     if (n == 0 || (p + n - 1) / n > kMaxDigitBits) return false;
     if (is_small_length(n)) return 2 * (p / n) >= (uint64_t)ceil_log2(n) + 4;
-    const int l = ilog2_exact(n);
-    if (l > kSmallLogMax && large_length_supported(l)) return 4 * (p / n) >= (uint64_t)l + 12;
+    if (large_fp64_length(n)) return 4 * (p / n) >= (uint64_t)ceil_log2(n) + 12;
     return false;
 }
 
@@ -490,9 +498,11 @@ struct SplitInit {
 int shape_log_c(int v) { return v < 0 ? -1 : v & 0xff; }
 int shape_rows(int v) { return v < 0 ? 0 : v >> 8; }
 
-cudaError_t init_large(LargeTest& T, uint64_t p, int l) {
+cudaError_t init_large(LargeTest& T, uint64_t p, uint64_t n) {
+    const int l = ilog2_exact(n);
+    if (l < 0) return T.init(p, n);  // R0 2^k: fixed shape
     const int v = g_large_shape[l].load();
-    return T.init(p, l, shape_log_c(v), shape_rows(v));
+    return T.init(p, n, shape_log_c(v), shape_rows(v));
 }
 
 // The autotuner's choices (llgpu.autotune) persist in a text file, one line per choice:
@@ -528,7 +538,7 @@ void load_tuning_once(int dev) {
         std::fclose(f);
     });
 }
-cudaError_t init_large(NttLargeTest& T, uint64_t p, int l) { return T.init(p, l); }
+cudaError_t init_large(NttLargeTest& T, uint64_t p, uint64_t n) { return T.init(p, ilog2_exact(n)); }
 
 // The exact residue of a two-pass test's digits (on the device after its FINAL pass), rebuilt on
 // the GPU; the words come back to the host only when asked for (into a vector or a caller buffer).
@@ -589,7 +599,7 @@ int run_large_t(const Item& item, llg_result& r, std::vector<uint64_t>* words, c
         return bail(fail(LLG_E_NOMEM, "allocating the residue snapshot"));
     for (;;) {
         TestT T;
-        cudaError_t ce = init_large(T, p, ilog2_exact(n));
+        cudaError_t ce = init_large(T, p, n);
         if (ce == cudaSuccess) ce = cudaEventRecord(e0, st);
         if (ce == cudaSuccess) {
             if (snap_iters == 0) {
@@ -1156,7 +1166,7 @@ struct llg_test {
     std::unique_ptr<llg::NttLargeTest> n;  // NTT engine
     int dev = -1;
     uint64_t p() const { return f ? f->p : n->p; }
-    int logN() const { return f ? f->logN : n->logN; }
+    uint64_t len() const { return f ? f->N : n->N; }
     uint64_t done() const { return f ? f->done : n->done; }
 };
 
@@ -1174,7 +1184,7 @@ int llg_test_create(uint64_t p, uint32_t n, int engine, llg_test** out) {
     if (n == 0) n = ntt ? ntt_len(p) : fp64_length(p, g_max_bpw);
     const int l = ilog2_exact(n);
     const bool ok = ntt ? (l > kSmallLogMax && ntt_large_length_supported(l) && ntt_length_usable(p, n))
-                        : (l > kSmallLogMax && large_length_supported(l) && fp64_length_usable(p, n));
+                        : (large_fp64_length(n) && fp64_length_usable(p, n));
     if (!ok)
         return fail(LLG_E_UNSUPPORTED, "length %u not usable by the two-pass %s engine for p=%llu", n,
                     ntt ? "NTT" : "FP64", (unsigned long long)p);
@@ -1186,7 +1196,7 @@ int llg_test_create(uint64_t p, uint32_t n, int engine, llg_test** out) {
         e = t->n->init(p, l);
     } else {
         t->f.reset(new llg::LargeTest());
-        e = init_large(*t->f, p, l);
+        e = init_large(*t->f, p, n);
     }
     if (e != cudaSuccess) {
         delete t;
@@ -1199,7 +1209,7 @@ int llg_test_create(uint64_t p, uint32_t n, int engine, llg_test** out) {
 int llg_test_start(llg_test* t, void* stream) {
     if (!t) return fail(LLG_E_ARG, "null test");
     cudaStream_t st = stream ? (cudaStream_t)stream : default_stream_for_thread();
-    const std::vector<int> seed = seed_digits(1ull << t->logN());
+    const std::vector<int> seed = seed_digits(t->len());
     if (t->f) CK(t->f->start(seed, st));
     else CK(t->n->start(seed, st));
     return LLG_OK;
@@ -1230,7 +1240,7 @@ int llg_test_read(llg_test* t, void* stream, llg_result* out, uint64_t* words, s
     std::memset(out, 0, sizeof *out);
     out->p = p;
     out->iters = t->done();
-    out->n = 1u << t->logN();
+    out->n = (uint32_t)t->len();
     out->max_err = bits_to_double(h.err_max);
     if (h.timeout) return fail(LLG_E_TIMEOUT, "carry wait timed out");
     int32_t z = 0;
@@ -1261,7 +1271,7 @@ int llg_test_load(llg_test* t, const uint64_t* words, size_t nwords, uint64_t it
     CK(cudaMallocAsync(&dw, nw * sizeof(uint64_t), st));
     cudaError_t e = cudaMemcpyAsync(dw, words, nw * sizeof(uint64_t), cudaMemcpyHostToDevice, st);
     int* digits = t->f ? t->f->digits : t->n->digits;
-    if (e == cudaSuccess) e = digits_from_words(p, 1ull << t->logN(), dw, digits, st);
+    if (e == cudaSuccess) e = digits_from_words(p, t->len(), dw, digits, st);
     if (e == cudaSuccess) e = t->f ? t->f->start_device(st) : t->n->start_device(st);
     cudaFreeAsync(dw, st);
     if (e != cudaSuccess) return fail(LLG_E_CUDA, "CUDA: %s", cudaGetErrorString(e));

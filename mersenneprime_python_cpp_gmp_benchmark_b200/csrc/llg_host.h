@@ -13,6 +13,8 @@ namespace llg {
 constexpr int kGraphChunk = 64;  // squarings per captured CUDA graph
 
 bool large_length_supported(int log_n);
+// N = R0 2^k two-pass lengths (R0 = 3, 5; k = 18 .. 21): R0 and the log2 row length they use.
+bool large_mixed_length_supported(uint64_t n, int* r0, int* log_c);
 int large_default_log_c(int log_n);
 bool large_split_supported(int log_n, int log_c, int rows);
 int set_error(int code, const char* msg);  // records this thread's llg_last_error() text
@@ -26,8 +28,9 @@ double2 padded_quarter_slot(uint64_t L, uint64_t i);
 std::vector<double2> spread_quarter_table(uint64_t L);
 
 struct LargeTest {
-    uint64_t p = 0, M = 0;
-    int logN = 0, logC = 0, logR = 0, C = 0, R = 0, rows = 0, nblocks = 0;
+    uint64_t p = 0, N = 0, M = 0;
+    // logN: log2 N (-1 for N = R0 2^k); logR: large_col_code of the column length R
+    int logN = 0, logC = 0, logR = 0, C = 0, R = 0, rows = 0, nblocks = 0, r0 = 1;
     double2* V = nullptr;
     double* carry = nullptr;
     double* carry2 = nullptr;
@@ -36,7 +39,7 @@ struct LargeTest {
     int* digits = nullptr;
     float* errlog = nullptr;
     int errlog_len = 0;
-    double2 *qtwC = nullptr, *qtwR = nullptr, *tw1 = nullptr, *tw2 = nullptr;
+    double2 *qtwC = nullptr, *qtwR = nullptr, *qtwL = nullptr, *tw1 = nullptr, *tw2 = nullptr;
     int* pos_of_c = nullptr;
     double *wA = nullptr, *iwA = nullptr, *wB = nullptr, *iwB = nullptr;
     int *sA = nullptr, *sB = nullptr;
@@ -45,8 +48,9 @@ struct LargeTest {
     uint64_t done = 0;  // squarings enqueued since start()
 
     ~LargeTest();
-    // log_c < 0: the default split; rows == 0: the default rows per row-pass block
-    cudaError_t init(uint64_t p, int log_n, int log_c = -1, int rows = 0);
+    // n: the transform length (2^14 .. 2^23, or R0 2^k as large_mixed_length_supported); log_c < 0:
+    // the default split; rows == 0: the default rows per row-pass block (power-of-two lengths)
+    cudaError_t init(uint64_t p, uint64_t n, int log_c = -1, int rows = 0);
     cudaError_t start(const std::vector<int>& digits, cudaStream_t st);  // INIT + first squaring
     cudaError_t start_device(cudaStream_t st);  // the same from the digits already in `digits`
     cudaError_t step(uint64_t k, cudaStream_t st);                        // k more squarings

@@ -144,7 +144,9 @@ __device__ __forceinline__ void wait_flag(unsigned int* f, unsigned int target, 
 struct LargeArgs {
     double2* V;               // state: element (row a, column slot pos) at pos * R + a
     const double2* qtwC;      // full padded twiddle table of the C-point row FFT
-    const double2* qtwR;      // quarter table of the R-point column FFT
+    const double2* qtwR;      // quarter table of the R-point column FFT (spread layout for a
+                              // power-of-two R, padded for R = R0 L)
+    const double2* qtwL;      // R = R0 L: padded quarter table of the L-point column sub-FFTs
     const double2* tw1;       // e^{-2 pi i x / M}, x < 2^tw_shift
     const double2* tw2;       // e^{-2 pi i y 2^tw_shift / M}
     const int* pos_of_c;      // column slot of row-FFT frequency c
@@ -167,11 +169,15 @@ struct LargeArgs {
     int tw_shift;
     int C, R, nblocks;
     int q, rem;               // p / N, p % N
-    int logN;
+    int N;                    // transform length: 2^k, or 3 x 2^k / 5 x 2^k (R = R0 L)
+    int logN;                 // log2 N for a power of two
 };
 
 // Row pass; grid > 0 overrides the block count (nblocks, + 1 for the wrap-around job unless INIT).
 cudaError_t launch_large_row(int log_c, int g, int mode, const LargeArgs& a, cudaStream_t st, int grid = 0);
+// Column-length code of the two-pass engine: log2 R for a power of two, 100 R0 + log2 L for the
+// column length R = R0 L (launch_large_col and configure_large take it).
+constexpr int large_col_code(int r0, int log_l) { return r0 == 1 ? log_l : 100 * r0 + log_l; }
 cudaError_t launch_large_col(int log_r, const LargeArgs& a, cudaStream_t st);
 
 // ---- two-pass exact NTT engine (N = 2^14 .. 2^23): N field elements in HBM ------------------

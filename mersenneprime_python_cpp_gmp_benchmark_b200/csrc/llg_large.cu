@@ -88,13 +88,14 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blo
     double2* qtw = xbuf + large_row_slots(LOG_C, G);               // padded twiddle table (C-point)
     double* swB = reinterpret_cast<double*>(qtw + QL);             // C column weights 2^(sB/N)
     double* siwB = swB + C;                                        // C inverse column weights
+    int* ssB = reinterpret_cast<int*>(siwB + C);                   // C column weight exponents sB
     __shared__ unsigned long long s_err;
     __shared__ int s_job;
     __shared__ unsigned s_epoch;
 
     const int t = threadIdx.x, ra = t % G, tr = t / G;
     double2* buf = xbuf + ra;
-    const int N = 1 << A.logN, R = A.R;
+    const int N = A.N, R = A.R;
     const CtaSync sync;
 
     if (t == 0) {
@@ -119,15 +120,14 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blo
     const unsigned ep = s_epoch;
     const bool wrap_job = job < 0;
     const int a = (wrap_job ? R - G : job * G) + ra;  // this thread's row
-    // weight exponent s = (sA(2a+e) + sB(b)) mod N of digit 2m+e; sB(b) = (-2 R b p) mod N from
-    // 32-bit products (N <= 2^23 < 2^32). digit_kind(b) gives bit 0 / 1: digit 0 / 1 of (a, b) has
+    // weight exponent s = (sA(2a+e) + sB(b)) mod N of digit 2m+e, sB(b) = (-2 R b p) mod N from
+    // the shared-memory copy of its table. digit_kind(b) gives bit 0 / 1: digit 0 / 1 of (a, b) has
     // q + 1 bits (s < p mod N); bit 2 / 3: sA + sB wrapped past N, so the weight 2^(s/N) is the
     // table product times 1/2 (and the inverse weight times 2). Recomputed where used: a few
     // integer operations, fewer live registers than keeping them.
     const int sA0 = __ldg(A.sA + 2 * a), sA1 = __ldg(A.sA + 2 * a + 1);
-    const uint32_t kB = (uint32_t)(2 * R) * (uint32_t)A.rem;
     auto digit_kind = [&](int b) {
-        const int sb = (int)((0u - kB * (uint32_t)b) & (uint32_t)(N - 1));
+        const int sb = ssB[b];
         const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
         const int s0 = o0 ? sA0 + sb - N : sA0 + sb, s1 = o1 ? sA1 + sb - N : sA1 + sb;
         return (uint32_t)(s0 < A.rem) | ((uint32_t)(s1 < A.rem) << 1) | ((uint32_t)o0 << 2) | ((uint32_t)o1 << 3);
@@ -142,7 +142,10 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blo
             v[i] = make_double2((double)d.x, (double)d.y);
         }
         for (int k = t; k < QL; k += T) qtw[k] = A.qtwC[k];
-        for (int k = t; k < C; k += T) swB[k] = __ldg(A.wB + k);
+        for (int k = t; k < C; k += T) {
+            swB[k] = __ldg(A.wB + k);
+            ssB[k] = __ldg(A.sB + k);
+        }
         __syncthreads();
     } else {
         // ---- the tile's rows, straight into registers: thread (row, tr) holds positions
@@ -158,6 +161,7 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blo
         for (int k = t; k < C; k += T) {
             swB[k] = __ldg(A.wB + k);
             siwB[k] = __ldg(A.iwB + k);
+            ssB[k] = __ldg(A.sB + k);
         }
         __syncthreads();
         inverse_from<GC, GC::P - 1, false, CtaSync, G, LE>(v, buf, qtw, tr, sync);
@@ -498,7 +502,7 @@ __global__ void __launch_bounds__(2 * R0 * (1 << LOG_L) / (1 << kLargeLogE), (2 
 template <int LOG_C, int G>
 static size_t row_smem() {
     using GC = SmallG<LOG_C, large_row_log_e(LOG_C, G), TW_FULL>;
-    return sizeof(double2) * (large_row_slots(LOG_C, G) + twiddle_table_len<GC>()) + 2 * sizeof(double) * GC::M;
+    return sizeof(double2) * (large_row_slots(LOG_C, G) + twiddle_table_len<GC>()) + (2 * sizeof(double) + sizeof(int)) * GC::M;
 }
 
 template <int LOG_R>
@@ -515,6 +519,16 @@ static int carveout_pct(size_t bytes, int blocks) {
     const int pct = (int)((100 * need + 228 * 1024 - 1) / (228 * 1024));
     return pct > 100 ? 100 : pct;
 }
+
+template <int R0, int LOG_L>
+static size_t col_mixed_smem() {
+    using GL = SmallGeom<LOG_L, kLargeLogE>;
+    constexpr int L = GL::M, R = R0 * L;
+    return sizeof(double2) * (2 * R0 * GL::PAD + qpad_len(L / 4) + qpad_len(R / 4) + 2 * R0 * R0 + 2 * GL::E);
+}
+
+template <int R0, int LOG_L>
+constexpr int col_mixed_threads() { return 2 * R0 * (1 << LOG_L) / (1 << kLargeLogE); }
 
 template <int LOG_C, int G, int MODE>
 static cudaError_t row_attr() {
@@ -542,6 +556,22 @@ static cudaError_t col_attr() {
         e = cudaFuncSetAttribute(large_col<LOG_R>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  carveout_pct(col_smem<LOG_R>(), LOG_R <= 11 ? 2 : 1));
     return e;
+}
+
+template <int R0, int LOG_L>
+static cudaError_t col_mixed_attr() {
+    cudaError_t e = cudaFuncSetAttribute(large_col_mixed<R0, LOG_L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)col_mixed_smem<R0, LOG_L>());
+    if (!e)
+        e = cudaFuncSetAttribute(large_col_mixed<R0, LOG_L>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 carveout_pct(col_mixed_smem<R0, LOG_L>(), col_mixed_threads<R0, LOG_L>() <= 256 ? 2 : 1));
+    return e;
+}
+
+template <int R0, int LOG_L>
+static cudaError_t col_mixed_t(const LargeArgs& a, cudaStream_t st) {
+    large_col_mixed<R0, LOG_L><<<a.C / 2 + 1, col_mixed_threads<R0, LOG_L>(), col_mixed_smem<R0, LOG_L>(), st>>>(a);
+    return cudaGetLastError();
 }
 
 // INIT: one block per tile. ITER / FINAL: one block more, for the wrap-around job (grid == 0), or
@@ -572,6 +602,8 @@ cudaError_t configure_large(int log_c, int g, int log_r) {
     }
     if (e) return e;
     switch (log_r) {
+        case large_col_code(3, 9): return col_mixed_attr<3, 9>();
+        case large_col_code(5, 9): return col_mixed_attr<5, 9>();
         case 7: return col_attr<7>();
         case 8: return col_attr<8>();
         case 9: return col_attr<9>();
@@ -604,6 +636,8 @@ cudaError_t launch_large_row(int log_c, int g, int mode, const LargeArgs& a, cud
 
 cudaError_t launch_large_col(int log_r, const LargeArgs& a, cudaStream_t st) {
     switch (log_r) {
+        case large_col_code(3, 9): return col_mixed_t<3, 9>(a, st);
+        case large_col_code(5, 9): return col_mixed_t<5, 9>(a, st);
         case 7: return col_t<7>(a, st);
         case 8: return col_t<8>(a, st);
         case 9: return col_t<9>(a, st);

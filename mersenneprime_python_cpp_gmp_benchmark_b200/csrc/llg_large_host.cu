@@ -98,6 +98,24 @@ cudaError_t upload(T** d, const std::vector<T>& h) {
 
 bool large_length_supported(int log_n) { return log_n >= 14 && log_n <= 23; }
 
+// The non-power-of-two two-pass lengths N = R0 2^k (R0 = 3, 5; k = 18 .. 21): columns of
+// R = R0 2^9 complex values (large_col_mixed), rows of 2^(k - 10). Below k = 18 the C / 2 + 1
+// column-pair blocks (65 or fewer) leave most of the GPU idle and the next power of two is faster.
+bool large_mixed_length_supported(uint64_t n, int* r0, int* log_c) {
+    for (int r = 3; r <= 5; r += 2) {
+        if (n % (uint64_t)r) continue;
+        const uint64_t m = n / (uint64_t)r;
+        if (m & (m - 1)) continue;
+        int k = 0;
+        while ((1ull << k) < m) ++k;
+        if (k < 18 || k > 21) return false;
+        if (r0) *r0 = r;
+        if (log_c) *log_c = k - 10;
+        return true;
+    }
+    return false;
+}
+
 // Row length (2^log_c complex values) of the two-pass FP64 engine at N = 2^log_n by default.
 int large_default_log_c(int log_n) {
     return (log_n <= 15) ? log_n - 8 : (log_n <= 17) ? 8 : (log_n <= 19) ? 9 : 10;
@@ -113,32 +131,55 @@ bool large_split_supported(int log_n, int log_c, int rows) {
 
 LargeTest::~LargeTest() {
     if (exec) cudaGraphExecDestroy(exec);
-    void* ptrs[] = {V, carry, carry2, ctl, flags, digits, errlog, qtwC, qtwR, tw1, tw2, pos_of_c, wA, iwA, sA, wB, iwB, sB};
+    void* ptrs[] = {V, carry, carry2, ctl, flags, digits, errlog, qtwC, qtwR, qtwL, tw1, tw2, pos_of_c, wA, iwA, sA, wB, iwB, sB};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
 
-cudaError_t LargeTest::init(uint64_t p_, int log_n, int log_c, int rows_) {
+cudaError_t LargeTest::init(uint64_t p_, uint64_t n, int log_c, int rows_) {
     p = p_;
-    logN = log_n;
-    const uint64_t N = 1ull << logN;
+    N = n;
     M = N / 2;
-    logC = large_default_log_c(logN);
-    if (log_c >= 0) logC = log_c;
-    rows = rows_ ? rows_ : large_rows_per_block(logC);
-    if (!large_split_supported(logN, logC, rows)) return cudaErrorInvalidValue;
-    logR = logN - 1 - logC;
-    C = 1 << logC;
-    R = 1 << logR;
+    int mixed_log_c = 0;
+    if (large_mixed_length_supported(N, &r0, &mixed_log_c)) {
+        // R = R0 2^9 columns, rows of M / R (the row shape is fixed: no autotuned split here)
+        logN = -1;
+        logC = mixed_log_c;
+        rows = large_rows_per_block(logC);
+        if (!large_rows_supported(logC, rows)) return cudaErrorInvalidValue;
+        C = 1 << logC;
+        R = (int)(M / (uint64_t)C);
+        logR = large_col_code(r0, 9);
+    } else {
+        r0 = 1;
+        logN = 0;
+        while ((1ull << logN) < N) ++logN;
+        if ((1ull << logN) != N) return cudaErrorInvalidValue;
+        logC = large_default_log_c(logN);
+        if (log_c >= 0) logC = log_c;
+        rows = rows_ ? rows_ : large_rows_per_block(logC);
+        if (!large_split_supported(logN, logC, rows)) return cudaErrorInvalidValue;
+        logR = logN - 1 - logC;
+        C = 1 << logC;
+        R = 1 << logR;
+    }
     nblocks = R / rows;
-    const int s = std::max(logC, (int)((logN - 1 + 1) / 2));
+    int log_m = 0;
+    while ((1ull << log_m) < M) ++log_m;
+    // four-step twiddles w_M^x, x = a c < M, as tw1[x mod 2^s] tw2[x >> s]
+    const int s = std::max(logC, (log_m + 1) / 2);
     cudaError_t e;
     if ((e = configure_large(logC, rows, logR))) return e;
     // tables
     if ((e = upload(&qtwC, padded_full_table(C)))) return e;
-    if ((e = upload(&qtwR, spread_quarter_table(R)))) return e;  // the column pass reads qpad_s
+    if (r0 == 1) {
+        if ((e = upload(&qtwR, spread_quarter_table(R)))) return e;  // the column pass reads qpad_s
+    } else {
+        if ((e = upload(&qtwR, padded_quarter_table(R)))) return e;    // R = R0 2^9 (twiddle_r)
+        if ((e = upload(&qtwL, padded_quarter_table(R / r0)))) return e;
+    }
     if ((e = upload(&tw1, omega_table(M, 1ull << s, 1)))) return e;
-    if ((e = upload(&tw2, omega_table(M, M >> s, 1ull << s)))) return e;
+    if ((e = upload(&tw2, omega_table(M, (M + (1ull << s) - 1) >> s, 1ull << s)))) return e;
     std::vector<int> pc(C);
     for (int c = 0; c < C; ++c) pc[c] = host_pos_of_freq(logC, large_row_log_e(logC, rows), c);
     if ((e = upload(&pos_of_c, pc))) return e;
@@ -182,6 +223,7 @@ cudaError_t LargeTest::init(uint64_t p_, int log_n, int log_c, int rows_) {
     A.V = V;
     A.qtwC = qtwC;
     A.qtwR = qtwR;
+    A.qtwL = qtwL;
     A.tw1 = tw1;
     A.tw2 = tw2;
     A.pos_of_c = pos_of_c;
@@ -204,8 +246,9 @@ cudaError_t LargeTest::init(uint64_t p_, int log_n, int log_c, int rows_) {
     A.C = C;
     A.R = R;
     A.nblocks = nblocks;
-    A.q = (int)(p >> logN);
-    A.rem = (int)(p & (N - 1));
+    A.q = (int)(p / N);
+    A.rem = (int)(p % N);
+    A.N = (int)N;
     A.logN = logN;
     return cudaSuccess;
 }

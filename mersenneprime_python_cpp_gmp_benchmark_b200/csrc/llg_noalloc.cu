@@ -241,6 +241,7 @@ extern "C" int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* 
     A.nblocks = R / kTileRows;
     A.q = (int)(p >> logN);
     A.rem = (int)(p & (N - 1));
+    A.N = (int)N;
     A.logN = logN;
 
     // s_0 = 4 as digits (the output buffer doubles as the INIT input), control block cleared.

@@ -371,3 +371,66 @@ def test_withheld_wrap_times_out_and_engine_recovers(gpu, oracle):
     t.close()
     r = gpu.run(p, iters=240, n=n)
     assert r["status"] == 0 and r["res64"] == _after()[(p, 240)]
+
+
+# ---- the {3, 5} x 2^k two-pass lengths (columns of R0 x 512 complex) ---------------------------
+
+MIXED_LARGE = [r << k for r in (3, 5) for k in range(18, 22)]
+
+
+@pytest.mark.parametrize("n", MIXED_LARGE)
+def test_mixed_large_length_full_residue(gpu, oracle, n):
+    """Every two-pass length R0 x 2^k at its fewest usable bits per digit (the longest carry
+    chains relative to the digit size, and the cheapest oracle run), full residue past the first
+    wrap-around."""
+    b = -(-((n - 1).bit_length() + 12) // 4)  # 4 floor(p/N) >= ceil(log2 N) + 12
+    p = _odd_candidate(b * n + n // 3)
+    k = p.bit_length() + 4
+    r = gpu.run(p, iters=k, n=n, want_words=True)
+    assert r["status"] == 0 and r["n"] == n and r["iters"] == k
+    assert r["words"] == oracle.ll_gmp(p, k)[2]
+
+
+@pytest.mark.parametrize("n", [3 << 18, 5 << 18, 3 << 19])
+def test_mixed_large_length_typical_digits(gpu, oracle, n):
+    """The same lengths at ~17 bits per digit, where the round-off is largest, over enough
+    squarings for the residue to be random."""
+    p = _odd_candidate(17 * n + 12345)
+    k = 40
+    r = gpu.run(p, iters=k, n=n, want_words=True)
+    assert r["status"] == 0 and r["n"] == n and r["escalations"] == 0 and r["max_err"] < 0.4
+    assert r["words"] == oracle.ll_gmp(p, k)[2]
+
+
+def test_sweep_primes_at_their_own_length(gpu):
+    """The 8 seeded primes of [20M, 25M] at the engine's default length (<= 18 bits per digit):
+    5 x 2^18 or 3 x 2^19 instead of 2^21, no escalation, round-off <= 0.4, res64 after 1000
+    squarings equal to the reference GMP engine's."""
+    g = load_json("appendix.json")
+    after = _after()
+    for p in g["sweep_primes"]:
+        r = gpu.run(p, iters=1000)
+        assert r["status"] == 0 and r["n"] <= 3 << 19 and r["n"] in (5 << 18, 3 << 19), (p, r["n"])
+        assert r["escalations"] == 0 and r["max_err"] <= 0.4, (p, r["max_err"])
+        assert r["res64"] == after[(p, 1000)], p
+
+
+def test_mixed_large_load_and_interim(gpu, oracle):
+    """llg_test_* at a mixed length: pieces equal one run, a residue loaded from 2^20 resumes at
+    5 x 2^18 bit-exactly."""
+    p = 20357693
+    t = gpu.Test(p, 1 << 21)
+    t.start()
+    t.iterate(99)
+    w = t.read(want_words=True)["words"]
+    t.close()
+    m = gpu.Test(p, 5 << 18)
+    m.load(w, 100)
+    m.iterate(49)
+    mid = m.read()
+    m.iterate(50)
+    r = m.read(want_words=True)
+    m.close()
+    assert mid["iters"] == 150 and r["iters"] == 200 and r["n"] == 5 << 18
+    assert r["res64"] == gpu.run(p, iters=200, n=5 << 18)["res64"]
+    assert mid["res64"] == gpu.run(p, iters=150, n=1 << 21)["res64"]
