@@ -119,6 +119,30 @@ __device__ __forceinline__ double2 twiddle_g(const double2* __restrict__ q, uint
     }
 }
 
+// vv[k1] *= w^{x k1} (conjugated when INV) for k1 = 1 .. R-1, w = e^{-2 pi i / M}, x = n2 2^(LE S).
+// Every twiddle read from the table, or (G::TWF, R >= 8) only those of k1 = 1, 2, 3 and
+// k1 = 4, 8, 12 (R = 16; 4 for R = 8), the others formed as one product w^{x (k1 mod 4)}
+// w^{x (k1 - k1 mod 4)}: 6 (4) table reads instead of 15 (7), each product within about an ulp.
+template <class G, int R, bool INV>
+__device__ __forceinline__ void apply_twiddles(double2* vv, const double2* __restrict__ qtw, uint32_t x) {
+    if constexpr (G::TWF && R >= 8) {
+        double2 lo[4], hi[4];
+#pragma unroll
+        for (int k = 1; k < 4; ++k) lo[k] = twiddle_g<G>(qtw, x * (uint32_t)k, INV);
+#pragma unroll
+        for (int k = 1; k < R / 4; ++k) hi[k] = twiddle_g<G>(qtw, x * (uint32_t)(4 * k), INV);
+#pragma unroll
+        for (int k1 = 1; k1 < R; ++k1) {
+            const int l = k1 & 3, h = k1 >> 2;
+            const double2 w = h == 0 ? lo[l] : (l == 0 ? hi[h] : cmul(hi[h], lo[l]));
+            vv[k1] = cmul(vv[k1], w);
+        }
+    } else {
+#pragma unroll
+        for (int k1 = 1; k1 < R; ++k1) vv[k1] = cmul(vv[k1], twiddle_g<G>(qtw, x * (uint32_t)k1, INV));
+    }
+}
+
 // Forward (INV=false) or inverse radix pass S on the register array v (E values).
 // Forward: load (S > 0), DFT, twiddle w_L^{n2 k1}, store (S < P-1).
 // Inverse: load (S < P-1), conj twiddle, inverse DFT, store (S > 0).
@@ -157,17 +181,9 @@ __device__ __forceinline__ void radix_pass(double2 (&v)[G::E], double2* __restri
         }
         if constexpr (!INV) {
             Dft<R, false>::run(vv);
-            if constexpr (ST > 1) {
-#pragma unroll
-                for (int k1 = 1; k1 < R; ++k1)
-                    vv[k1] = cmul(vv[k1], twiddle_g<G>(qtw, (uint32_t)(n2 * k1) << (G::LE * S), false));
-            }
+            if constexpr (ST > 1) apply_twiddles<G, R, false>(vv, qtw, (uint32_t)n2 << (G::LE * S));
         } else {
-            if constexpr (ST > 1) {
-#pragma unroll
-                for (int k1 = 1; k1 < R; ++k1)
-                    vv[k1] = cmul(vv[k1], twiddle_g<G>(qtw, (uint32_t)(n2 * k1) << (G::LE * S), true));
-            }
+            if constexpr (ST > 1) apply_twiddles<G, R, true>(vv, qtw, (uint32_t)n2 << (G::LE * S));
             Dft<R, true>::run(vv);
         }
         if constexpr (STORE && !SYNC_BEFORE_STORE) {
@@ -219,10 +235,12 @@ __device__ __forceinline__ void inverse_from(double2 (&v)[G::E], double2* buf, c
     }
 }
 
-template <int LOG_M_T, int LOG_E = 4, int TW = TW_QUARTER>
+// TF: the radix passes form their twiddles from fewer table reads (apply_twiddles).
+template <int LOG_M_T, int LOG_E = 4, int TW = TW_QUARTER, bool TF = false>
 struct SmallG : SmallGeom<LOG_M_T, LOG_E> {
     static constexpr int LOG_M_ = LOG_M_T;
     static constexpr int TWM = TW;
+    static constexpr bool TWF = TF;
 };
 
 // Length (16-byte slots) of the twiddle table a geometry reads.

@@ -40,7 +40,7 @@ __host__ __device__ constexpr int small_log_e(int log_m) { return log_m == 9 ? 3
 // reads and the real-FFT split's digit-reversed reads conflict most in the qpad layout
 __host__ __device__ constexpr int small_tw_layout(int log_m) { return log_m >= 10 ? TW_QUARTER_S : TW_QUARTER; }
 template <int LOG_M>
-using SmallGeo = SmallG<LOG_M, small_log_e(LOG_M), small_tw_layout(LOG_M)>;
+using SmallGeo = SmallG<LOG_M, small_log_e(LOG_M), small_tw_layout(LOG_M), true>;
 
 bool small_fp64_spread_table(int log_n) { return small_tw_layout(log_n - 1) == TW_QUARTER_S; }
 // blocks per SM the kernel is built for: 128 registers a thread at 16 values, ~85 at 8

@@ -33,7 +33,7 @@ namespace {
 // passes than with 16 (L = 2^9: 8 x 8 x 8 against 16 x 16 x 2), else 16
 template <int R0_, int LOG_L, int LE_ = (LOG_L == 9 ? 3 : 4)>
 struct MixedGeom {
-    using GL = SmallG<LOG_L, LE_, TW_QUARTER>;
+    using GL = SmallG<LOG_L, LE_, TW_QUARTER, true>;
     static constexpr int R0 = R0_;
     static constexpr int L = GL::M, TL = GL::T, E = GL::E;
     static constexpr int M = R0 * L, N = 2 * M, T = R0 * TL;
