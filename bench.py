@@ -210,6 +210,9 @@ def bench_range(args, rank, world):
     import torch
     from mersenneprime_python_cpp_gmp_benchmark_b200 import llgpu
     ps_all = sieve(2, RANGE_HI)
+    # the range autotuner picks, per whole-test length of the bits-per-digit rule, the fastest of
+    # that length and the next usable ones on this GPU (power of two against {3,5} x 2^k)
+    tuned = llgpu.autotune_range(RANGE_HI, save=False)
     from mersenneprime_python_cpp_gmp_benchmark_b200 import replicas
     mine = replicas.shard(ps_all, rank, world)  # independent tests, balanced by squaring cost
     batch = llgpu.Batch(mine)
@@ -261,6 +264,8 @@ def bench_range(args, rank, world):
                                "N = {1,3,5} x 2^k from 32 to 6144 at <=18 bits/digit)",
                    "lengths": {str(n): c for n, c in sorted(__import__("collections").Counter(r["n"] for r in res).items())},
                    "tests": len(ps_all), "l2": "flushed (512 MiB write) between steps",
+                   "autotuned_lengths": {str(n): {"use": best, "candidates_ms": {str(c): round(v, 2) for c, v in t.items()}}
+                                         for n, (best, t) in tuned.items()},
                    "parallelism": f"independent tests split over {world} GPU(s) by squaring cost (replicas)"},
         "e2e": {"value": round(e2e, 2), "unit": "tests/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "fp64", "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "TFLOP/s",

@@ -83,6 +83,14 @@ uint32_t llg_ntt_length(uint64_t p);
  * per block in *rows (may be null). */
 int llg_set_large_split(int log_n, int log_c, int rows);
 int llg_get_large_split(int log_n, int* rows);
+/* Length choice for whole-test exponents: where the bits-per-digit rule of llg_fft_length gives
+ * the whole-test length n_rule, use n_use (>= n_rule; 0 or n_rule: the rule's own) for exponents it
+ * is usable for. The range autotuner (llgpu.autotune_range) times the candidates per length and
+ * sets the fastest; the tune file of llg_set_large_split also keeps these. No reference counterpart
+ * (the reference always takes the smallest {1,3,5} x 2^k length, lucaslehmer.cpp:244-254).
+ * llg_get_length_choice returns the length used where the rule gives n_rule. */
+int llg_set_length_choice(uint32_t n_rule, uint32_t n_use);
+uint32_t llg_get_length_choice(uint32_t n_rule);
 /* Largest exponent an engine handles. Replaces max_exponent(), cuda/ll_ntt.cu:279. */
 uint64_t llg_max_exponent(int engine);
 

@@ -225,9 +225,26 @@ bool fp64_length_usable(uint64_t p, uint64_t n) {
 }
 
 // smallest usable length with p / N <= bpw
+// Length choices of the autotuner (llg_set_length_choice): where the bits-per-digit rule gives a
+// whole-test length N, use the recorded length instead (when usable for p). Indexed by N's
+// position in fp64_lengths(); 0 = the rule's own length.
+constexpr size_t kMaxLengths = 64;
+std::atomic<uint32_t> g_length_choice[kMaxLengths];
+
+int length_index(uint32_t n) {
+    const std::vector<uint32_t>& v = fp64_lengths();
+    for (size_t i = 0; i < v.size() && i < kMaxLengths; ++i)
+        if (v[i] == n) return (int)i;
+    return -1;
+}
+
 uint32_t fp64_length(uint64_t p, double bpw) {
     for (uint32_t N : fp64_lengths())
-        if ((double)p / (double)N <= bpw && fp64_length_usable(p, N)) return N;
+        if ((double)p / (double)N <= bpw && fp64_length_usable(p, N)) {
+            const int i = length_index(N);
+            const uint32_t c = i >= 0 ? g_length_choice[i].load() : 0u;
+            return (c && fp64_length_usable(p, c)) ? c : N;
+        }
     return 0;
 }
 
@@ -505,8 +522,10 @@ cudaError_t init_large(LargeTest& T, uint64_t p, uint64_t n) {
     return T.init(p, n, shape_log_c(v), shape_rows(v));
 }
 
-// The autotuner's choices (llgpu.autotune) persist in a text file, one line per choice:
+// The autotuners' choices (llgpu.autotune, llgpu.autotune_range) persist in a text file, one line
+// per choice:
 //   large_split <TAB> device name <TAB> log2 N <TAB> log2 row length <TAB> rows per block
+//   length <TAB> device name <TAB> whole-test length of the rule <TAB> length to use instead
 // read once per process from $LLG_TUNE_CACHE, else $HOME/.cache/llgpu/tune.txt. Lines for other
 // devices or unsupported splits are ignored; llg_set_large_split overrides.
 void load_tuning_once(int dev) {
@@ -530,6 +549,13 @@ void load_tuning_once(int dev) {
             char* save = nullptr;
             for (char* tok = strtok_r(line, "\t\n", &save); tok && nf < 5; tok = strtok_r(nullptr, "\t\n", &save))
                 fields[nf++] = tok;
+            if (nf == 4 && std::strcmp(fields[0], "length") == 0 && std::strcmp(fields[1], prop.name) == 0) {
+                const uint32_t nd = (uint32_t)std::strtoul(fields[2], nullptr, 10);
+                const uint32_t nu = (uint32_t)std::strtoul(fields[3], nullptr, 10);
+                const int i = length_index(nd);
+                if (i >= 0 && is_small_length(nd) && length_index(nu) >= 0 && nu >= nd) g_length_choice[i].store(nu);
+                continue;
+            }
             if (nf != 5 || std::strcmp(fields[0], "large_split") != 0 || std::strcmp(fields[1], prop.name) != 0)
                 continue;
             const int ln = std::atoi(fields[2]), lc = std::atoi(fields[3]), rows = std::atoi(fields[4]);
@@ -1026,6 +1052,21 @@ int llg_get_large_split(int log_n, int* rows) {
     const int lc = v >= 0 ? shape_log_c(v) : large_default_log_c(log_n);
     if (rows) *rows = v >= 0 ? shape_rows(v) : large_rows_per_block(lc);
     return lc;
+}
+
+int llg_set_length_choice(uint32_t n_rule, uint32_t n_use) {
+    const int i = length_index(n_rule);
+    if (i < 0 || !is_small_length(n_rule)) return fail(LLG_E_ARG, "%u is not a whole-test FP64 length", n_rule);
+    if (n_use && (length_index(n_use) < 0 || n_use < n_rule))
+        return fail(LLG_E_ARG, "%u is not an FP64 length at least %u", n_use, n_rule);
+    g_length_choice[i].store(n_use == n_rule ? 0u : n_use);
+    return LLG_OK;
+}
+
+uint32_t llg_get_length_choice(uint32_t n_rule) {
+    const int i = length_index(n_rule);
+    const uint32_t c = i >= 0 ? g_length_choice[i].load() : 0u;
+    return c ? c : n_rule;
 }
 
 int llg_set_roundoff_limit(double limit) {

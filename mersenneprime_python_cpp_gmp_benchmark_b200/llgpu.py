@@ -54,6 +54,9 @@ def lib() -> ctypes.CDLL:
         L.llg_fft_length.restype = u32
         L.llg_set_max_bpw.argtypes = [dbl]
         L.llg_set_roundoff_limit.argtypes = [dbl]
+        L.llg_set_length_choice.argtypes = [u32, u32]
+        L.llg_get_length_choice.argtypes = [u32]
+        L.llg_get_length_choice.restype = u32
         L.llg_get_roundoff_limit.argtypes = []
         L.llg_get_roundoff_limit.restype = dbl
         L.llg_get_max_bpw.restype = dbl
@@ -136,6 +139,89 @@ def set_roundoff_limit(limit):
 
 def get_roundoff_limit():
     return lib().llg_get_roundoff_limit()
+
+
+def set_length_choice(n_rule, n_use):
+    """llg_set_length_choice: where the bits-per-digit rule gives the whole-test length n_rule, use
+    n_use (0: the rule's own)."""
+    _check(lib().llg_set_length_choice(n_rule, n_use))
+
+
+def get_length_choice(n_rule):
+    return lib().llg_get_length_choice(n_rule)
+
+
+def _usable_lengths(p, lo, count):
+    """The FP64 lengths >= lo usable for p, ascending (at most count): llg_fft_length at a falling
+    bits-per-digit bound walks up the ladder of lengths."""
+    out, bpw = [], p / lo
+    while len(out) < count and bpw > 2.0:
+        n = fft_length(p, bpw)
+        if n and n >= lo and n not in out:
+            out.append(n)
+        bpw *= 0.97
+    return sorted(out)
+
+
+def autotune_range(hi=100001, iters=1000, tests=444, candidates=3, save=True, path=None):
+    """Times, for every whole-test length N the bits-per-digit rule picks for the primes p <= hi,
+    a batch of that bucket's largest exponents (`tests` of them, one block each, `iters` squarings)
+    at N and at the next usable whole-test lengths (up to `candidates` in all), keeps the fastest
+    in force (llg_set_length_choice) and, with `save`, records it in the tune file.
+    Returns {N: (chosen, {candidate: device ms})}."""
+    name = device_info()[0]
+    buckets, old = {}, {}
+    for p in _primes(3, hi):
+        n = fft_length(p)
+        if n and n <= 12288:
+            buckets.setdefault(n, []).append(p)
+    for n in buckets:
+        old[n] = get_length_choice(n)
+        set_length_choice(n, 0)
+    out = {}
+    try:
+        for n, bp in sorted(buckets.items()):
+            sample = sorted(bp)[-tests:]
+            # whole-test lengths only (a two-pass length would run the bucket one exponent at a time)
+            cands = [c for c in _usable_lengths(sample[0], n, candidates) if c <= 12288]
+            times = {}
+            for c in cands:
+                set_length_choice(n, c)
+                b = Batch(sample, iters)
+                try:
+                    b.launch()
+                    b.device_ms()
+                    b.launch()
+                    times[c] = b.device_ms()
+                finally:
+                    b.close()
+            set_length_choice(n, 0)
+            out[n] = (min(times, key=times.get) if times else n, times)
+        for n, (best, _) in out.items():
+            set_length_choice(n, best)
+    except Exception:
+        for n, c in old.items():
+            set_length_choice(n, c)
+        raise
+    if save:
+        path = path or tune_cache_path()
+        keep = []
+        if os.path.exists(path):
+            with open(path) as f:
+                for line in f:
+                    fl = line.rstrip("\n").split("\t")
+                    if len(fl) >= 3 and fl[0] == "length" and fl[1] == name and int(fl[2]) in out:
+                        continue
+                    keep.append(line.rstrip("\n"))
+        os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
+        tmp = path + ".tmp"
+        with open(tmp, "w") as f:
+            for line in keep:
+                f.write(line + "\n")
+            for n, (best, _) in sorted(out.items()):
+                f.write(f"length\t{name}\t{n}\t{best}\n")
+        os.replace(tmp, path)
+    return out
 
 
 def set_large_split(log_n, log_c, rows=0):

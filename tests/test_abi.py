@@ -150,3 +150,23 @@ def test_tune_file_round_trip(tmp_path, monkeypatch):
     assert "large_split\tOther GPU\t23\t11\t2" in lines
     assert sum(1 for l in lines if l.startswith("large_split\tNVIDIA B200\t22\t")) == 1
     assert sum(1 for l in lines if l.startswith("large_split\tNVIDIA B200\t23\t")) == 1
+
+
+def test_length_choice_rule():
+    """llg_set_length_choice: exponents whose bits-per-digit length is n_rule move to n_use where
+    it is usable for them; clearing restores the rule; lengths shorter than the rule's, and
+    non-lengths, are refused."""
+    from mersenneprime_python_cpp_gmp_benchmark_b200 import llgpu
+    p = 85009  # 16.6 bits per digit at N = 5120, the rule's length
+    assert llgpu.fft_length(p) == 5120
+    try:
+        llgpu.set_length_choice(5120, 8192)
+        assert llgpu.get_length_choice(5120) == 8192
+        assert llgpu.fft_length(p) == 8192 and llgpu.fft_length(p, 17.0) == 8192
+        with pytest.raises(llgpu.LlgError):
+            llgpu.set_length_choice(5120, 4096)  # shorter than the rule's length
+        with pytest.raises(llgpu.LlgError):
+            llgpu.set_length_choice(5000, 8192)  # not a length
+    finally:
+        llgpu.set_length_choice(5120, 0)
+    assert llgpu.fft_length(p) == 5120 and llgpu.get_length_choice(5120) == 5120

@@ -181,3 +181,21 @@ def test_all_primes_to_100001_full_residues(gpu, oracle):
         if r["is_zero"]:
             hits.append(p)
     assert hits == [p for p in known_exponents() if p <= 100001]
+
+
+def test_range_autotuner_keeps_residues_exact(gpu):
+    """llgpu.autotune_range times each bucket's candidate lengths and puts the fastest in force;
+    with its choices every prime p <= 10001 still has the reference's residue, and clearing them
+    restores the rule's lengths."""
+    from conftest import load_range
+    gold = load_range()
+    out = gpu.autotune_range(hi=10001, iters=200, tests=148, save=False)
+    try:
+        assert out and all(best >= n for n, (best, _) in out.items())
+        ps = [p for p in sorted(gold) if p <= 10001]
+        res = gpu.run_batch(ps)
+        assert all((bool(r["is_zero"]), r["res64"]) == gold[r["p"]][:2] for r in res)
+    finally:
+        for n in out:
+            gpu.set_length_choice(n, 0)
+    assert all(gpu.get_length_choice(n) == n for n in out)
