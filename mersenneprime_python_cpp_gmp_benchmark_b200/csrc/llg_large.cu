@@ -281,7 +281,7 @@ template <int LOG_R>
 __global__ void __launch_bounds__(2 * (1 << LOG_R) / (1 << kLargeLogE), (LOG_R <= 11 ? 2 : 1)) large_col(const LargeArgs A) {
     // quarter twiddle table in the spread layout (entry r at qpad_s(r)): the strided twiddle reads
     // of the radix passes spread over more bank groups than with qpad
-    using GR = SmallG<LOG_R, kLargeLogE, TW_QUARTER_S>;
+    using GR = SmallG<LOG_R, kLargeLogE, TW_QUARTER_S, true>;
     constexpr int R = GR::M, TC = GR::T, E = GR::E;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2* bufs = reinterpret_cast<double2*>(smem_raw);  // 2 exchange buffers of PAD slots
