@@ -78,7 +78,7 @@ template <int LOG_C, int G, int MODE>
 __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blocks(LOG_C, G))
     large_row(const LargeArgs A) {
     constexpr int LE = large_row_log_e(LOG_C, G);
-    using GC = SmallG<LOG_C, LE, TW_FULL>;  // full twiddle table
+    using GC = SmallG<LOG_C, LE, TW_FULL, true>;  // full twiddle table, factored twiddles
     constexpr int C = GC::M, TR = GC::T, E = GC::E, T = G * TR;
     static_assert(T % 32 == 0 && 32 % G == 0, "whole warps of whole row groups");
     constexpr unsigned FULL = 0xffffffffu;
@@ -379,7 +379,7 @@ __device__ __forceinline__ double2 pair_term_r(double2 acc, double2 a, double2 b
 template <int R0, int LOG_L>
 __global__ void __launch_bounds__(2 * R0 * (1 << LOG_L) / (1 << kLargeLogE), (2 * R0 * (1 << LOG_L) / (1 << kLargeLogE) <= 256 ? 2 : 1))
     large_col_mixed(const LargeArgs A) {
-    using GL = SmallG<LOG_L, kLargeLogE>;
+    using GL = SmallG<LOG_L, kLargeLogE, TW_QUARTER, true>;
     constexpr int L = GL::M, TL = GL::T, E = GL::E, R = R0 * L, TC = R0 * TL, PADL = GL::PAD;
     constexpr int QLL = (int)qpad_len(L / 4), QLR = (int)qpad_len(R / 4);
     static_assert(TL % 32 == 0 && 2 * TC <= 1024, "whole warps per segment");
@@ -501,7 +501,7 @@ __global__ void __launch_bounds__(2 * R0 * (1 << LOG_L) / (1 << kLargeLogE), (2 
 
 template <int LOG_C, int G>
 static size_t row_smem() {
-    using GC = SmallG<LOG_C, large_row_log_e(LOG_C, G), TW_FULL>;
+    using GC = SmallG<LOG_C, large_row_log_e(LOG_C, G), TW_FULL, true>;
     return sizeof(double2) * (large_row_slots(LOG_C, G) + twiddle_table_len<GC>()) + (2 * sizeof(double) + sizeof(int)) * GC::M;
 }
 
