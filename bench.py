@@ -289,7 +289,13 @@ def bench_big(args, rank, world):
     from mersenneprime_python_cpp_gmp_benchmark_b200 import llgpu
     n = 1 << 23
     tuned = None
-    if args.engine == "fp64":
+    if args.engine == "fp64" and args.split:
+        # a fixed split (a profiler's timings would mislead the autotuner)
+        c, g = (int(x) for x in args.split.split(","))
+        llgpu.set_large_split(23, c, g)
+        tuned = {"row_length": f"2^{c} complex", "column_length": f"2^{22 - c} complex", "rows_per_block": g,
+                 "candidates_us": None, "fixed": True}
+    elif args.engine == "fp64":
         # the autotuner picks the row x column split of the two-pass engine on this GPU
         best, cand = llgpu.autotune([23], save=False)[23]
         tuned = {"row_length": f"2^{best[0]} complex", "column_length": f"2^{22 - best[0]} complex",
@@ -733,6 +739,9 @@ def main():
                     help="range: leave out the timing of the reference's own GPU engine")
     ap.add_argument("--no-range", action="store_true",
                     help="big: leave out the range sub-record (the other half of the metric)")
+    ap.add_argument("--split", default="",
+                    help="big, FP64: the two-pass split 'log2 row length,rows per block' instead of the "
+                         "autotuner's choice (e.g. 10,8)")
     args = ap.parse_args()
     threads = os.cpu_count() or 1
     if args.impl == "reference":

@@ -126,12 +126,19 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blo
     // table product times 1/2 (and the inverse weight times 2). Recomputed where used: a few
     // integer operations, fewer live registers than keeping them.
     const int sA0 = __ldg(A.sA + 2 * a), sA1 = __ldg(A.sA + 2 * a + 1);
-    auto digit_kind = [&](int b) {
+    auto kind_at = [&](int s0a, int s1a, int b) {
         const int sb = ssB[b];
-        const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
-        const int s0 = o0 ? sA0 + sb - N : sA0 + sb, s1 = o1 ? sA1 + sb - N : sA1 + sb;
+        const bool o0 = s0a + sb >= N, o1 = s1a + sb >= N;
+        const int s0 = o0 ? s0a + sb - N : s0a + sb, s1 = o1 ? s1a + sb - N : s1a + sb;
         return (uint32_t)(s0 < A.rem) | ((uint32_t)(s1 < A.rem) << 1) | ((uint32_t)o0 << 2) | ((uint32_t)o1 << 3);
     };
+    auto digit_kind = [&](int b) { return kind_at(sA0, sA1, b); };
+    // the digit kinds of this thread's E values, 4 bits each, from the carry to the re-weighting
+    // (at 16 values a thread; at 8, where registers are scarcer, recomputed)
+    constexpr bool KEEP_KINDS = LE >= 4;
+    uint32_t kinds[(E + 7) / 8];
+#pragma unroll
+    for (int w = 0; w < (E + 7) / 8; ++w) kinds[w] = 0u;
 
     double2 v[E];
     if constexpr (MODE == LARGE_INIT) {
@@ -178,6 +185,7 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blo
             const int b = tr + TR * i;
             const double iwb = siwB[b];
             const uint32_t kd = digit_kind(b);
+            if (KEEP_KINDS) kinds[i / 8] |= kd << (4 * (i % 8));
             const int w0 = kd & 1u, w1 = (kd >> 1) & 1u;
             const double va = v[i].x * (ia0 * iwb) * ((kd & 4u) ? 2.0 : 1.0);
             const double vb = v[i].y * (ia1 * iwb) * ((kd & 8u) ? 2.0 : 1.0);
@@ -220,26 +228,44 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blo
         }
         if (wrap_job) return;
         // ---- the tile's first row: hops 2 and 3 from the previous tile's last row (or the wrap);
-        //      its hop-2 carry-out is hop 3 of the second row ----
+        //      its hop-2 carry-outs are hop 3 of the second row. The row passes through the
+        //      exchange buffer (free until the forward FFT's first stores), so that every thread
+        //      takes E / G of its columns rather than one lane in G all of them. ----
+        double2* row0 = xbuf;                                    // C slots: row 0 of the tile
+        double* hop3 = reinterpret_cast<double*>(xbuf + C);      // C doubles: hop 3 into row 1
+        if (ra == 0) {
+#pragma unroll
+            for (int i = 0; i < E; ++i) row0[tr + TR * i] = v[i];
+        }
         if (t == 0) wait_flag(&A.flags[job], ep + 1u, A.ctl, A.spin_limit);
         __syncthreads();
-        const double* cprev = A.carry + (size_t)job * C;
-        const double* c2prev = A.carry2 + (size_t)job * C;
+        {
+            const int a0 = job * G;
+            const int s0a = __ldg(A.sA + 2 * a0), s1a = __ldg(A.sA + 2 * a0 + 1);
+            const double* cprev = A.carry + (size_t)job * C;
+            const double* c2prev = A.carry2 + (size_t)job * C;
+            static_assert(C % T == 0, "whole columns per thread");
 #pragma unroll
-        for (int i = 0; i < E; ++i) {
-            const int b = tr + TR * i;
-            double c2 = 0.0;
-            if (ra == 0) {
-                const uint32_t kd = digit_kind(b);
+            for (int k = 0; k < C / T; ++k) {
+                const int b = t + T * k;
+                const uint32_t kd = kind_at(s0a, s1a, b);
                 double cin = __ldcg(cprev + b);
-                if (a == 0 && b == 0) cin -= 2.0;  // the "- 2" of s^2 - 2 (digit 0)
-                double c;
-                const double x0 = dsplit_e(v[i].x + cin, A.q + (int)(kd & 1u), c);
-                const double x1 = dsplit_e(v[i].y + c, A.q + (int)((kd >> 1) & 1u), c2);
-                v[i] = make_double2(x0 + __ldcg(c2prev + b), x1);
+                if (job == 0 && b == 0) cin -= 2.0;  // the "- 2" of s^2 - 2 (digit 0)
+                const double2 x = row0[b];
+                double c, c2;
+                const double x0 = dsplit_e(x.x + cin, A.q + (int)(kd & 1u), c);
+                const double x1 = dsplit_e(x.y + c, A.q + (int)((kd >> 1) & 1u), c2);
+                row0[b] = make_double2(x0 + __ldcg(c2prev + b), x1);
+                hop3[b] = c2;
             }
-            const double up = __shfl_up_sync(FULL, c2, 1, G);
-            if (ra == 1) v[i].x += up;
+        }
+        __syncthreads();
+        if (ra == 0) {
+#pragma unroll
+            for (int i = 0; i < E; ++i) v[i] = row0[tr + TR * i];
+        } else if (ra == 1) {
+#pragma unroll
+            for (int i = 0; i < E; ++i) v[i].x += hop3[tr + TR * i];
         }
         if (MODE == LARGE_FINAL || A.dump) {
 #pragma unroll
@@ -256,11 +282,16 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blo
 #pragma unroll
     for (int i = 0; i < E; ++i) {
         const double wb = swB[tr + TR * i];
-        const uint32_t kd = digit_kind(tr + TR * i);
+        const uint32_t kd = (MODE == LARGE_INIT || !KEEP_KINDS) ? digit_kind(tr + TR * i) : (kinds[i / 8] >> (4 * (i % 8)));
         v[i].x *= (wa0 * wb) * ((kd & 4u) ? 0.5 : 1.0);
         v[i].y *= (wa1 * wb) * ((kd & 8u) ? 0.5 : 1.0);
     }
-    forward_from<GC, 0, CtaSync, G, LE>(v, buf, qtw, tr, sync);
+    // the first forward pass stores after a barrier: the first row's carry may still be read from
+    // the exchange buffer
+    radix_pass<GC, 0, false, true, CtaSync, G, LE>(v, buf, qtw, tr, sync);
+    static_assert(GC::P > 1, "at least two row-FFT passes");
+    sync();
+    forward_from<GC, 1, CtaSync, G, LE>(v, buf, qtw, tr, sync);
     if (MODE == LARGE_ITER && job == A.nblocks - 1) {
         // rows R-G .. R-1 are the wrap job's input: wait (bounded) until it has read them
         if (t == 0) wait_flag(&A.flags[0], ep + 1u, A.ctl, A.spin_limit);
