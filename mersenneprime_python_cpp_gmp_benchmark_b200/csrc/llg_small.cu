@@ -99,6 +99,29 @@ __global__ void __launch_bounds__(SmallGeo<LOG_M>::T, small_min_blocks(SmallGeo<
         iwA1 = exp2(-(double)sA1 / (double)N);
     }
 
+    // kind of the two digits of column i, fixed for the whole test, 4 bits per column: bit 0 / 1:
+    // digit 2m / 2m+1 has q + 1 bits (s < p mod N); bit 2 / 3: s_A + s_B wrapped past N (weight
+    // = table product / 2, inverse weight x 2)
+    uint32_t kinds[(E + 7) / 8];
+#pragma unroll
+    for (int w = 0; w < (E + 7) / 8; ++w) kinds[w] = 0u;
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+        const int sb = sB[i];
+        const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
+        const int s0 = o0 ? sA0 + sb - N : sA0 + sb;
+        const int s1 = o1 ? sA1 + sb - N : sA1 + sb;
+        const uint32_t kd = (uint32_t)(s0 < rem) | ((uint32_t)(s1 < rem) << 1) | ((uint32_t)o0 << 2) | ((uint32_t)o1 << 3);
+        kinds[i / 8] |= kd << (4 * (i % 8));
+    }
+    auto kind = [&](int i) { return kinds[i / 8] >> (4 * (i % 8)); };
+    // made opaque before each use: the weights and digit sizes derived from the kinds are then
+    // formed where used, not hoisted into registers held across the transforms
+    auto refresh_kinds = [&]() {
+#pragma unroll
+        for (int w = 0; w < (E + 7) / 8; ++w) asm volatile("" : "+r"(kinds[w]));
+    };
+
     double2 v[E];
     // s_0 = 4: digit 0 (thread 0, i = 0, even) has weight a_0 = 1
 #pragma unroll
@@ -148,20 +171,18 @@ __global__ void __launch_bounds__(SmallGeo<LOG_M>::T, small_min_blocks(SmallGeo<
         // unweight, round, error, local carry (even -> odd digit); the carry-out of column i goes
         // to thread t+1 (lane shuffle) or, at a warp boundary, through cbuf after the barrier
         double lerr = 0.0;
+        refresh_kinds();
         if (active) {
 #pragma unroll
             for (int i = 0; i < E; ++i) {
-                const int sb = sB[i];
-                const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
-                const int s0 = o0 ? sA0 + sb - N : sA0 + sb;
-                const int s1 = o1 ? sA1 + sb - N : sA1 + sb;
+                const uint32_t kd = kind(i);
                 const double iw = iwB[i];
-                const double a = v[i].x * (iwA0 * iw) * (o0 ? 2.0 : 1.0);
-                const double b = v[i].y * (iwA1 * iw) * (o1 ? 2.0 : 1.0);
+                const double a = v[i].x * (iwA0 * iw) * ((kd & 4u) ? 2.0 : 1.0);
+                const double b = v[i].y * (iwA1 * iw) * ((kd & 8u) ? 2.0 : 1.0);
                 long long la, lb;
                 const double ra = round_shift(a, la), rb = round_shift(b, lb);
                 lerr = fmax(lerr, fmax(fabs(a - ra), fabs(b - rb)));
-                const int b0 = q + (s0 < rem), b1 = q + (s1 < rem);  // digit sizes
+                const int b0 = q + (int)(kd & 1u), b1 = q + (int)((kd >> 1) & 1u);  // digit sizes
                 double c;
                 double x0 = dsplit_e(ra, b0, c);
                 const double x1 = dsplit_e(rb + c, b1, c);
@@ -184,17 +205,15 @@ __global__ void __launch_bounds__(SmallGeo<LOG_M>::T, small_min_blocks(SmallGeo<
             errlog[it] = (float)__longlong_as_double((long long)serr[it & 1]);
             serr[(it + 1) & 1] = 0ull;
         }
+        refresh_kinds();
         if (active && lane == 0) {
 #pragma unroll
             for (int i = 0; i < E; ++i) {
                 double cin = (warp > 0) ? cbuf[(warp - 1) * E + i]
                                         : cbuf[(W - 1) * E + ((i + E - 1) % E)];  // m-1 wraps at m=0
                 if (t == 0 && i == 0) cin -= 2.0;  // the "- 2" of s^2 - 2
-                const int sb = sB[i];
-                const bool o0 = sA0 + sb >= N;
-                const int s0 = o0 ? sA0 + sb - N : sA0 + sb;
                 double c;
-                x0s[i] = d2i_exact(dsplit_e((double)x0s[i] + cin, q + (s0 < rem), c));
+                x0s[i] = d2i_exact(dsplit_e((double)x0s[i] + cin, q + (int)(kind(i) & 1u), c));
                 x1s[i] += (int)c;
             }
         }
@@ -204,14 +223,14 @@ __global__ void __launch_bounds__(SmallGeo<LOG_M>::T, small_min_blocks(SmallGeo<
             break;
         }
         if (it >= iters) break;
+        refresh_kinds();
         if (active) {
 #pragma unroll
             for (int i = 0; i < E; ++i) {
-                const int sb = sB[i];
-                const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
+                const uint32_t kd = kind(i);
                 const double w = wB[i];
-                v[i].x = i2d_shift(x0s[i]) * (wA0 * w) * (o0 ? 0.5 : 1.0);
-                v[i].y = i2d_shift(x1s[i]) * (wA1 * w) * (o1 ? 0.5 : 1.0);
+                v[i].x = i2d_shift(x0s[i]) * (wA0 * w) * ((kd & 4u) ? 0.5 : 1.0);
+                v[i].y = i2d_shift(x1s[i]) * (wA1 * w) * ((kd & 8u) ? 0.5 : 1.0);
             }
         }
     }

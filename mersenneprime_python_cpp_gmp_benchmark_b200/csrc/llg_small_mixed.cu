@@ -132,6 +132,28 @@ __global__ void __launch_bounds__(MixedGeom<R0, LOG_L>::T, mixed_min_blocks(Mixe
     const double wA0 = exp2((double)sA0 / (double)N), wA1 = exp2((double)sA1 / (double)N);
     const double iwA0 = exp2(-(double)sA0 / (double)N), iwA1 = exp2(-(double)sA1 / (double)N);
 
+    // kind of the two digits of column i, fixed for the whole test, 4 bits per column: bit 0 / 1:
+    // digit 2m / 2m+1 has q + 1 bits; bit 2 / 3: its weight wrapped past N
+    uint32_t kinds[(E + 7) / 8];
+#pragma unroll
+    for (int w = 0; w < (E + 7) / 8; ++w) kinds[w] = 0u;
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+        const int sb = sB[i];
+        const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
+        const int s0 = o0 ? sA0 + sb - N : sA0 + sb;
+        const int s1 = o1 ? sA1 + sb - N : sA1 + sb;
+        const uint32_t kd = (uint32_t)(s0 < rem) | ((uint32_t)(s1 < rem) << 1) | ((uint32_t)o0 << 2) | ((uint32_t)o1 << 3);
+        kinds[i / 8] |= kd << (4 * (i % 8));
+    }
+    auto kind = [&](int i) { return kinds[i / 8] >> (4 * (i % 8)); };
+    // made opaque before each use: the weights and digit sizes derived from the kinds are then
+    // formed where used, not hoisted into registers held across the transforms
+    auto refresh_kinds = [&]() {
+#pragma unroll
+        for (int w = 0; w < (E + 7) / 8; ++w) asm volatile("" : "+r"(kinds[w]));
+    };
+
     // the carry into lane 0 of this warp comes from the last lane of warp `src`, column i - shift
     int src, wrapcol;
     if (wl > 0) {
@@ -220,19 +242,17 @@ __global__ void __launch_bounds__(MixedGeom<R0, LOG_L>::T, mixed_min_blocks(Mixe
 
         // ---- unweight, round, error, carry (as in the power-of-two kernel) ----
         double lerr = 0.0;
+        refresh_kinds();
 #pragma unroll
         for (int i = 0; i < E; ++i) {
-            const int sb = sB[i];
-            const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
-            const int s0 = o0 ? sA0 + sb - N : sA0 + sb;
-            const int s1 = o1 ? sA1 + sb - N : sA1 + sb;
+            const uint32_t kd = kind(i);
             const double iw = iwB[i];
-            const double a = v[i].x * (iwA0 * iw) * (o0 ? 2.0 : 1.0);
-            const double b = v[i].y * (iwA1 * iw) * (o1 ? 2.0 : 1.0);
+            const double a = v[i].x * (iwA0 * iw) * ((kd & 4u) ? 2.0 : 1.0);
+            const double b = v[i].y * (iwA1 * iw) * ((kd & 8u) ? 2.0 : 1.0);
             long long la, lb;
             const double ra = round_shift(a, la), rb = round_shift(b, lb);
             lerr = fmax(lerr, fmax(fabs(a - ra), fabs(b - rb)));
-            const int b0 = q + (s0 < rem), b1 = q + (s1 < rem);  // digit sizes
+            const int b0 = q + (int)(kd & 1u), b1 = q + (int)((kd >> 1) & 1u);  // digit sizes
             double c;
             double x0 = dsplit_e(ra, b0, c);
             const double x1 = dsplit_e(rb + c, b1, c);
@@ -254,6 +274,7 @@ __global__ void __launch_bounds__(MixedGeom<R0, LOG_L>::T, mixed_min_blocks(Mixe
             errlog[it] = (float)__longlong_as_double((long long)serr[it & 1]);
             serr[(it + 1) & 1] = 0ull;
         }
+        refresh_kinds();
         if (lane == 0) {
 #pragma unroll
             for (int i = 0; i < E; ++i) {
@@ -261,11 +282,8 @@ __global__ void __launch_bounds__(MixedGeom<R0, LOG_L>::T, mixed_min_blocks(Mixe
                 if (!wrapcol) cin = cbuf[src * E + i];
                 else cin = (i > 0) ? cbuf[src * E + i - 1] : cbuf[src0 * E + E - 1];
                 if (t == 0 && i == 0) cin -= 2.0;  // the "- 2" of s^2 - 2
-                const int sb = sB[i];
-                const bool o0 = sA0 + sb >= N;
-                const int s0 = o0 ? sA0 + sb - N : sA0 + sb;
                 double c;
-                x0s[i] = d2i_exact(dsplit_e((double)x0s[i] + cin, q + (s0 < rem), c));
+                x0s[i] = d2i_exact(dsplit_e((double)x0s[i] + cin, q + (int)(kind(i) & 1u), c));
                 x1s[i] += (int)c;
             }
         }
@@ -275,13 +293,13 @@ __global__ void __launch_bounds__(MixedGeom<R0, LOG_L>::T, mixed_min_blocks(Mixe
             break;
         }
         if (it >= iters) break;
+        refresh_kinds();
 #pragma unroll
         for (int i = 0; i < E; ++i) {
-            const int sb = sB[i];
-            const bool o0 = sA0 + sb >= N, o1 = sA1 + sb >= N;
+            const uint32_t kd = kind(i);
             const double w = wB[i];
-            v[i].x = i2d_shift(x0s[i]) * (wA0 * w) * (o0 ? 0.5 : 1.0);
-            v[i].y = i2d_shift(x1s[i]) * (wA1 * w) * (o1 ? 0.5 : 1.0);
+            v[i].x = i2d_shift(x0s[i]) * (wA0 * w) * ((kd & 4u) ? 0.5 : 1.0);
+            v[i].y = i2d_shift(x1s[i]) * (wA1 * w) * ((kd & 8u) ? 0.5 : 1.0);
         }
     }
 
