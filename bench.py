@@ -54,9 +54,9 @@ STEP_ITERS = 1000  # squarings per timed step of the p=136,279,841 workload
 PASS_ITERS = 100   # squarings timed pass by pass for the dominant kernel's roofline
 # DRAM bytes (read + write) of one launch at p=136,279,841, N=2^23, from an ncu capture of
 # `python -m mersenneprime_python_cpp_gmp_benchmark_b200.llgpu square --p 136279841 --n 8388608
-# --iters 6` (NTT: `... --iters 6 --engine ntt`). ncu captures run cold (caches flushed), so these
-# are upper bounds on a warm launch, where part of the 64 MiB state is still in L2.
-NCU_TRAFFIC = {"fp64": {"row": 106451200, "column": 78296064},
+# --iters 6 --shape 10,8` (NTT: `... --iters 6 --engine ntt`). ncu captures run cold (caches
+# flushed), so these are upper bounds on a warm launch, where part of the 64 MiB state is still in L2.
+NCU_TRAFFIC = {"fp64": {"row": 89817600, "column": 76730880},
                "ntt": {"row": 115433728, "column": 94066176}}
 
 
