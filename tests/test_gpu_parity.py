@@ -67,13 +67,13 @@ def test_batch_matches_single(gpu):
         assert rb["res64"] == rs["res64"] and rb["n"] == rs["n"]
 
 
-def test_roundoff_escalation_stays_exact(gpu, oracle):
-    """Force a length far too short (27 bits per digit: the convolution outgrows FP64's 53 bits):
-    the kernel must abort on round-off, the host must redo it at a longer length on the GPU, and
-    the residue must still be exact."""
-    p = 27611
-    r = gpu.run(p, iters=300, n=1024, want_words=True)
-    assert r["status"] == 0 and r["escalations"] >= 1 and r["n"] > 1024
+@pytest.mark.parametrize("p,n", [(27611, 1024), (138239, 5120)])
+def test_roundoff_escalation_stays_exact(gpu, oracle, p, n):
+    """Force a length far too short (27 bits per digit: the convolution outgrows FP64's 53 bits),
+    a power of two and a 5 x 2^k length: the kernel must abort on round-off, the host must redo it
+    at a longer length on the GPU, and the residue must still be exact."""
+    r = gpu.run(p, iters=300, n=n, want_words=True)
+    assert r["status"] == 0 and r["escalations"] >= 1 and r["n"] > n
     assert r["words"] == oracle.ll_gmp(p, 300)[2]
 
 
