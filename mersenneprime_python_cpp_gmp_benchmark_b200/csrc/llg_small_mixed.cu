@@ -331,22 +331,25 @@ __global__ void __launch_bounds__(MixedGeom<R0, LOG_L>::T, mixed_min_blocks(Mixe
 
 // ---- the same transform with the radix-R0 steps in registers ----
 //
-// Between squarings, and for the radix-R0 steps and the carry, thread t < TA = L / 2 holds
-// x[c] = u[t + TA c], c < CA = 2 R0: both columns n = t and n = t + TA of every segment r
-// (c = i + 2 r, n = t + TA i). The radix-R0 DFT of column n is then in one thread's registers;
+// Between squarings, and for the radix-R0 steps and the carry, thread t < TA = L / NPT holds
+// x[c] = u[t + TA c], c < CA = NPT R0: the NPT columns n = t + TA i of every segment r
+// (c = i + NPT r). The radix-R0 DFT of column n is then in one thread's registers;
 // one store and one load per value move it to and from the segment-major order of the L-point
 // FFTs (thread (seg, tl) holds z[seg][tl + TL i]). The layout above reads R0 values from shared
 // memory for every output of each radix-R0 step instead. The digit order m = t + TA c runs
 // across the lanes, then to the next column, as in the power-of-two kernel, so the carry is that
-// kernel's with TA threads and CA columns. Used where the FFTs' R0 segments take at least TA
-// threads (R0 = 5, L = 2^9: 320 threads, of which 256 hold digits).
+// kernel's with TA threads and CA columns. The FFTs' R0 segments take at least TA threads:
+// R0 = 5, L = 2^9: 320 threads, 256 of them hold 2 columns; R0 = 3, L = 2^9: 192 threads, 128
+// of them hold 4 columns.
 template <int R0_, int LOG_L>
 struct MixedRGeom {
     using GL = SmallG<LOG_L, 3, TW_QUARTER, true>;
     static constexpr int R0 = R0_;
     static constexpr int L = GL::M, TL = GL::T, E = GL::E;
     static constexpr int M = R0 * L, N = 2 * M;
-    static constexpr int TA = L / 2, CA = 2 * R0, WA = TA / 32;
+    static constexpr int NPT = R0 == 5 ? 2 : 4;  // columns n per digit thread
+    static constexpr int MINB = R0 == 5 ? 2 : 4;  // blocks per SM the kernel is built for
+    static constexpr int TA = L / NPT, CA = NPT * R0, WA = TA / 32;
     static constexpr int T = R0 * TL, W = T / 32;
     static constexpr int PADL = GL::PAD;
     static constexpr int QLL = (int)qpad_len((uint32_t)L / 4);
@@ -385,14 +388,14 @@ __device__ __forceinline__ void dft_r0(double2 (&x)[R0], const double2* __restri
 }
 
 template <int R0, int LOG_L>
-__global__ void __launch_bounds__(MixedRGeom<R0, LOG_L>::T, 2)
+__global__ void __launch_bounds__(MixedRGeom<R0, LOG_L>::T, MixedRGeom<R0, LOG_L>::MINB)
     ll_small_fp64_mixed_r(const SmallJob* __restrict__ jobs, const double2* __restrict__ qtwL_g,
                           const double2* __restrict__ qtwM_g, int64_t* __restrict__ digits_out,
                           SmallResult* __restrict__ results, float* __restrict__ errlog, double abort_err) {
     using MG = MixedRGeom<R0, LOG_L>;
     using GL = typename MG::GL;
     constexpr int L = MG::L, TL = MG::TL, E = MG::E, M = MG::M, N = MG::N, T = MG::T, TA = MG::TA,
-                  CA = MG::CA, WA = MG::WA, PADL = MG::PADL, QLL = MG::QLL, QLM = MG::QLM;
+                  CA = MG::CA, WA = MG::WA, NPT = MG::NPT, PADL = MG::PADL, QLL = MG::QLL, QLM = MG::QLM;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2* bufs = reinterpret_cast<double2*>(smem_raw);  // R0 segment buffers of PADL slots
     double2* qtwL = bufs + R0 * PADL;                        // L-point quarter table
@@ -404,6 +407,7 @@ __global__ void __launch_bounds__(MixedRGeom<R0, LOG_L>::T, 2)
     double* cbuf = iwB + CA;                                 // WA * CA carry-outs of last lanes
     int* sB = reinterpret_cast<int*>(cbuf + WA * CA);
     unsigned long long* serr = reinterpret_cast<unsigned long long*>(sB + CA);  // 2 (8-aligned: CA even)
+    static_assert(CA % 2 == 0, "8-byte alignment of serr");
 
     const int t = threadIdx.x;
     const bool holds = t < TA;  // a digit thread (whole warps)
@@ -479,12 +483,12 @@ __global__ void __launch_bounds__(MixedRGeom<R0, LOG_L>::T, 2)
         refresh_kinds();
         if (holds) {
 #pragma unroll
-            for (int i = 0; i < 2; ++i) {
+            for (int i = 0; i < NPT; ++i) {
                 const int n = t + TA * i;
                 double2 z[R0];
 #pragma unroll
                 for (int r = 0; r < R0; ++r) {
-                    const int c = i + 2 * r;
+                    const int c = i + NPT * r;
                     const uint32_t kd = kind(c);
                     const double w = wB[c];
                     z[r] = make_double2(i2d_shift(x0s[c]) * (wA0 * w) * ((kd & 4u) ? 0.5 : 1.0),
@@ -544,7 +548,7 @@ __global__ void __launch_bounds__(MixedRGeom<R0, LOG_L>::T, 2)
         refresh_kinds();
         if (holds) {
 #pragma unroll
-            for (int i = 0; i < 2; ++i) {
+            for (int i = 0; i < NPT; ++i) {
                 const int n = t + TA * i;
                 double2 z[R0];
 #pragma unroll
@@ -552,7 +556,7 @@ __global__ void __launch_bounds__(MixedRGeom<R0, LOG_L>::T, 2)
                 dft_r0<R0>(z, omi);
 #pragma unroll
                 for (int r = 0; r < R0; ++r) {
-                const int c = i + 2 * r;
+                const int c = i + NPT * r;
                 const uint32_t kd = kind(c);
                 const double iw = iwB[c];
                 const double a = z[r].x * (iwA0 * iw) * ((kd & 4u) ? 2.0 : 1.0);
@@ -697,7 +701,7 @@ cudaError_t launch_small_fp64_mixed(uint32_t n, const SmallJob* jobs, int njobs,
     if (!mixed_length_supported(n, &r0, &l)) return cudaErrorInvalidValue;
     if (r0 == 3) {
         switch (l) {
-            case 9: return launch_mixed_t<3, 9>(jobs, njobs, qtwL, qtwM, digits, results, errlog, abort_err, st);
+            case 9: return launch_mixed_r_t<3, 9>(jobs, njobs, qtwL, qtwM, digits, results, errlog, abort_err, st);
             case 10: return launch_mixed_t<3, 10>(jobs, njobs, qtwL, qtwM, digits, results, errlog, abort_err, st);
             case 11: return launch_mixed_t<3, 11>(jobs, njobs, qtwL, qtwM, digits, results, errlog, abort_err, st);
         }
