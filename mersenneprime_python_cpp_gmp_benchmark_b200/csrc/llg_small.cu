@@ -64,6 +64,9 @@ __global__ void __launch_bounds__(SmallGeo<LOG_M>::T, small_min_blocks(SmallGeo<
     int* sB = reinterpret_cast<int*>(iwB + E);
     double* cbuf = reinterpret_cast<double*>(sB + E + (E & 1 ? 1 : 0) + 2);  // W * E
     unsigned long long* serr = reinterpret_cast<unsigned long long*>(cbuf + W * E);  // 2
+    // slot of the partner U_{M-k} of this thread's position t E + j, [j][t]: fixed for the whole
+    // test, read in the real-FFT split instead of two digit reversals a value
+    unsigned short* pslot = reinterpret_cast<unsigned short*>(serr + 2);  // E * T
 
     const int t = threadIdx.x;  // blockDim.x == T (a partial warp when T < 32)
     constexpr bool active = true;
@@ -85,6 +88,11 @@ __global__ void __launch_bounds__(SmallGeo<LOG_M>::T, small_min_blocks(SmallGeo<
         iwB[i] = exp2(-(double)s / (double)N) / (4.0 * (double)M);
     }
     for (int i = t; i < 2; i += T) serr[i] = 0ull;
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+        const int kp = (M - freq_of_pos<G>(t * E + j)) & (M - 1);
+        pslot[j * T + t] = (unsigned short)phys(pos_of_freq<G>(kp));
+    }
     __syncthreads();
 
     // per-thread weight halves for the even (e=0) and odd (e=1) digit of each u_m
@@ -155,9 +163,7 @@ __global__ void __launch_bounds__(SmallGeo<LOG_M>::T, small_min_blocks(SmallGeo<
             for (int h = 0; h < NB; ++h) wk[h] = twiddle_g<G>(qtw, (uint32_t)freq_rev<G>(t * NB + h), false);
 #pragma unroll
             for (int j = 0; j < E; ++j) {
-                const int k = freq_of_pos<G>(t * E + j);
-                const int kp = (M - k) & (M - 1);
-                const int x = phys(pos_of_freq<G>(kp));
+                const int x = pslot[j * T + t];
                 const double2 A = v[j], Bc = conj2(buf[x]);  // conj(U_{M-k})
                 const double2 s = cadd(A, Bc), d = csub(A, Bc);
                 const double2 a3 = make_double2(3.0 * A.x - Bc.x, 3.0 * A.y - Bc.y);
@@ -366,6 +372,7 @@ static size_t small_smem_bytes() {
     b += sizeof(double2) * twiddle_table_len<G>();
     b += 2 * sizeof(double) * G::E + sizeof(int) * (G::E + (G::E & 1 ? 1 : 0) + 2);
     b += sizeof(double) * G::W * G::E + 2 * sizeof(unsigned long long);
+    b += sizeof(unsigned short) * G::E * G::T;  // partner slots of the real-FFT split
     return b;
 }
 

@@ -340,15 +340,16 @@ __global__ void __launch_bounds__(MixedGeom<R0, LOG_L>::T, mixed_min_blocks(Mixe
 // across the lanes, then to the next column, as in the power-of-two kernel, so the carry is that
 // kernel's with TA threads and CA columns. The FFTs' R0 segments take at least TA threads:
 // R0 = 5, L = 2^9: 320 threads, 256 of them hold 2 columns; R0 = 3, L = 2^9: 192 threads, 128
-// of them hold 4 columns.
+// of them hold 4 columns; R0 = 3, L = 2^10 (16 values per FFT thread): 192 threads, 128 of them
+// hold 8 columns.
 template <int R0_, int LOG_L>
 struct MixedRGeom {
-    using GL = SmallG<LOG_L, 3, TW_QUARTER, true>;
+    using GL = SmallG<LOG_L, LOG_L == 9 ? 3 : 4, TW_QUARTER, true>;
     static constexpr int R0 = R0_;
     static constexpr int L = GL::M, TL = GL::T, E = GL::E;
     static constexpr int M = R0 * L, N = 2 * M;
-    static constexpr int NPT = R0 == 5 ? 2 : 4;  // columns n per digit thread
-    static constexpr int MINB = R0 == 5 ? 2 : 4;  // blocks per SM the kernel is built for
+    static constexpr int NPT = R0 == 5 ? 2 : (LOG_L == 9 ? 4 : 8);  // columns n per digit thread
+    static constexpr int MINB = (R0 == 5 || LOG_L > 9) ? 2 : 4;      // blocks per SM the kernel is built for
     static constexpr int TA = L / NPT, CA = NPT * R0, WA = TA / 32;
     static constexpr int T = R0 * TL, W = T / 32;
     static constexpr int PADL = GL::PAD;
@@ -408,6 +409,9 @@ __global__ void __launch_bounds__(MixedRGeom<R0, LOG_L>::T, MixedRGeom<R0, LOG_L
     int* sB = reinterpret_cast<int*>(cbuf + WA * CA);
     unsigned long long* serr = reinterpret_cast<unsigned long long*>(sB + CA);  // 2 (8-aligned: CA even)
     static_assert(CA % 2 == 0, "8-byte alignment of serr");
+    // slot of the partner U_{M-k} of position tl E + j of this thread's segment, [j][t]: fixed for
+    // the whole test, read in the real-FFT split instead of two digit reversals a value
+    unsigned short* pslot = reinterpret_cast<unsigned short*>(serr + 2);  // E * T
 
     const int t = threadIdx.x;
     const bool holds = t < TA;  // a digit thread (whole warps)
@@ -437,6 +441,15 @@ __global__ void __launch_bounds__(MixedRGeom<R0, LOG_L>::T, MixedRGeom<R0, LOG_L
         iwB[c] = exp2(-(double)s / (double)N) / (4.0 * (double)M);
     }
     if (t < 2) serr[t] = 0ull;
+    {
+        const int sg = t / TL, tq = t % TL, sgp = (sg == 0) ? 0 : R0 - sg;
+#pragma unroll
+        for (int j = 0; j < E; ++j) {
+            const int kk = freq_of_pos<GL>(tq * E + j);
+            const int kp = (sg == 0) ? ((L - kk) & (L - 1)) : (L - 1 - kk);
+            pslot[j * T + t] = (unsigned short)(sgp * PADL + phys(pos_of_freq<GL>(kp)));
+        }
+    }
     __syncthreads();
 
     const int sA0 = (int)(((uint64_t)N - ((uint64_t)(2 * t) * p) % (uint64_t)N) % (uint64_t)N);
@@ -515,7 +528,6 @@ __global__ void __launch_bounds__(MixedRGeom<R0, LOG_L>::T, MixedRGeom<R0, LOG_L
         for (int j = 0; j < E; ++j) mybuf[phys(tl * E + j)] = v[j];
         __syncthreads();
         {
-            const int segp = (seg == 0) ? 0 : R0 - seg;
             constexpr int RL = GL::RLAST, NB = E / RL;
             double2 wk[NB];
 #pragma unroll
@@ -523,10 +535,7 @@ __global__ void __launch_bounds__(MixedRGeom<R0, LOG_L>::T, MixedRGeom<R0, LOG_L
                 wk[h] = twiddle_m<M>(qtwM, (uint32_t)(R0 * freq_rev<GL>(tl * NB + h) + seg), false);
 #pragma unroll
             for (int j = 0; j < E; ++j) {
-                const int kk = freq_of_pos<GL>(tl * E + j);
-                const int kp = (seg == 0) ? ((L - kk) & (L - 1)) : (L - 1 - kk);
-                const int xi = segp * PADL + phys(pos_of_freq<GL>(kp));
-                const double2 A = v[j], Bc = conj2(bufs[xi]);  // conj(U_{M-k})
+                const double2 A = v[j], Bc = conj2(bufs[pslot[j * T + t]]);  // conj(U_{M-k})
                 const double2 s = cadd(A, Bc), d = csub(A, Bc);
                 const double2 a3 = make_double2(3.0 * A.x - Bc.x, 3.0 * A.y - Bc.y);
                 const double2 d2 = make_double2((d.x - d.y) * (d.x + d.y), 2.0 * d.x * d.y);
@@ -639,7 +648,8 @@ template <int R0, int LOG_L>
 static size_t mixed_r_smem_bytes() {
     using MG = MixedRGeom<R0, LOG_L>;
     return sizeof(double2) * ((size_t)R0 * MG::PADL + MG::QLL + MG::QLM + 2 * R0 * R0) +
-           sizeof(double) * (2 * MG::CA + MG::WA * MG::CA) + sizeof(int) * MG::CA + 2 * sizeof(unsigned long long);
+           sizeof(double) * (2 * MG::CA + MG::WA * MG::CA) + sizeof(int) * MG::CA + 2 * sizeof(unsigned long long) +
+           sizeof(unsigned short) * MG::E * MG::T;  // partner slots of the real-FFT split
 }
 
 template <int R0, int LOG_L>
@@ -702,7 +712,7 @@ cudaError_t launch_small_fp64_mixed(uint32_t n, const SmallJob* jobs, int njobs,
     if (r0 == 3) {
         switch (l) {
             case 9: return launch_mixed_r_t<3, 9>(jobs, njobs, qtwL, qtwM, digits, results, errlog, abort_err, st);
-            case 10: return launch_mixed_t<3, 10>(jobs, njobs, qtwL, qtwM, digits, results, errlog, abort_err, st);
+            case 10: return launch_mixed_r_t<3, 10>(jobs, njobs, qtwL, qtwM, digits, results, errlog, abort_err, st);
             case 11: return launch_mixed_t<3, 11>(jobs, njobs, qtwL, qtwM, digits, results, errlog, abort_err, st);
         }
     } else {
