@@ -242,15 +242,16 @@ def bench_range(args, rank, world):
     # e2e through the reference-facing call (host lists in, results out)
     import lucaslehmer_cuda as lc
     lc.lucas_lehmer_batch(mine[:64])
+    h0 = llgpu.h2d_bytes()
     t0 = time.perf_counter()
     out = lc.lucas_lehmer_batch(mine)
     t_e2e = time.perf_counter() - t0
+    h2d = llgpu.h2d_bytes() - h0
     assert sorted(p for p, r, s, res64 in out if r) == hits
     t_e2e = max_over_ranks(t_e2e, world)
     e2e = sum_over_ranks(len(mine), world) / t_e2e
-    # up: the job list (p, iterations) per test; back: its result record, res64 and zero flag (the
-    # residue is rebuilt on the device)
-    h2d = 16 * len(mine)
+    # up: measured by the library's count (the job lists and word offsets); back: each test's
+    # result record, res64 and zero flag (the residue is rebuilt on the device)
     d2h = (32 + 8 + 4) * len(mine)
     flops = range_flops(res)
     achieved = flops / (t_rank / args.steps) / 1e12
@@ -341,13 +342,22 @@ def bench_big(args, rank, world):
     # e2e: the reference-facing call, host in / host out, for a 2000-squaring interim residue
     import lucaslehmer as ll
     k_e2e = 2000
-    t0 = time.perf_counter()
-    if args.engine == "fp64":
-        res64, err = ll.fft_res64_after(BIG_P, k_e2e)
-    else:
-        res64 = ll.gmp_res64_after(BIG_P, k_e2e)  # the exact call; the NTT engine serves it
-    t_e2e = time.perf_counter() - t0
-    t_e2e = max_over_ranks(t_e2e, world)
+
+    def e2e_call():
+        h0 = llgpu.h2d_bytes()
+        t0 = time.perf_counter()
+        if args.engine == "fp64":
+            ll.fft_res64_after(BIG_P, k_e2e)
+        else:
+            ll.gmp_res64_after(BIG_P, k_e2e)  # the exact call; the NTT engine serves it
+        return max_over_ranks(time.perf_counter() - t0, world), llgpu.h2d_bytes() - h0
+
+    # a cold call (the two-pass test kept by the check run above released first: tables built and
+    # uploaded, buffers allocated, graphs captured inside the timed call), then the same call again
+    llgpu.release_cached()
+    t_e2e, h2d_e2e = e2e_call()
+    reps = [e2e_call() for _ in range(3)]
+    t_rep, h2d_rep = statistics.median(x[0] for x in reps), max(x[1] for x in reps)
     bytes_iter = 32.0 * n   # two read+write sweeps of the 8N-byte state
     bytes_pass = 16.0 * n   # one pass reads and writes the 8N-byte state once
     flops_iter = 5.0 * n * 23
@@ -378,10 +388,15 @@ def bench_big(args, rank, world):
                    "parallelism": f"one independent test per GPU ({world} replica(s))"},
         "e2e": {"value": round(1e6 * t_e2e / k_e2e, 3), "unit": "us/iteration", "iters": k_e2e,
                 "call": ("lucaslehmer.fft_res64_after" if args.engine == "fp64" else "lucaslehmer.gmp_res64_after")
-                        + "(136279841, 2000): tables, s_0 upload, squarings, exact residue rebuilt on the "
-                          "device, res64 back",
-                # s_0 as N int32 digits up; res64, the rebuild's flags and the control block back
-                "h2d_bytes_per_step": 4 * n, "d2h_bytes_per_step": 128},
+                        + "(136279841, 2000), cold: tables built and uploaded, buffers allocated, s_0 set on "
+                          "the device, graphs captured, squarings, exact residue rebuilt on the device, res64 back",
+                # measured by the library's own count (llg_h2d_bytes); back: res64, the rebuild's flags
+                # and the control block
+                "h2d_bytes_per_step": h2d_e2e, "d2h_bytes_per_step": 128,
+                "repeat_call": {"value": round(1e6 * t_rep / k_e2e, 3), "unit": "us/iteration",
+                                "h2d_bytes": h2d_rep,
+                                "note": "the same call again, median of 3: the two-pass test the previous "
+                                        "call kept (tables, buffers, graphs) is reused"}},
         "roofline": {"bound": "hbm", "achieved": round(bytes_pass / (dom_us * 1e-6) / 1e9, 1), "peak": hbm_peak,
                      "unit": "GB/s", "frac": round(bytes_pass / (dom_us * 1e-6) / 1e9 / hbm_peak, 4),
                      "peak_source": peak_source,
@@ -471,9 +486,12 @@ def bench_single(args, rank, world):
     # e2e: the C-ABI call llg_run at the same length for an interim residue, host in / host out
     k_e2e = 100000
     llgpu.run(p, iters=1000, n=SINGLE_N, engine=args.engine)
+    llgpu.release_cached()  # a cold call: tables and buffers inside the timed region
+    h0 = llgpu.h2d_bytes()
     t0 = time.perf_counter()
     e2e_r = llgpu.run(p, iters=k_e2e, n=SINGLE_N, engine=args.engine)
     t_e2e = max_over_ranks(time.perf_counter() - t0, world)
+    h2d_e2e = llgpu.h2d_bytes() - h0
     assert e2e_r["iters"] == k_e2e and e2e_r["n"] == SINGLE_N, e2e_r
     return {
         "metric": METRIC_SINGLE, "value": round(us_iter, 3), "unit": "us/iteration", "n_gpus": world,
@@ -489,7 +507,7 @@ def bench_single(args, rank, world):
         "e2e": {"value": round(1e6 * t_e2e / k_e2e, 3), "unit": "us/iteration", "iters": k_e2e,
                 "call": f"llg_run(1257787, {k_e2e}, {args.engine}, n=65536) through the C-ABI: tables, s_0 upload, "
                         "squarings, residue rebuilt on the device, result struct back",
-                "h2d_bytes_per_step": 4 * SINGLE_N, "d2h_bytes_per_step": 128},
+                "h2d_bytes_per_step": h2d_e2e, "d2h_bytes_per_step": 128},
         "clocks": clk.summary(),
         "gpu_launches": 2 * (p - 2),  # the reported engine's row and column pass per squaring
     }
@@ -508,7 +526,7 @@ def bench_sweep(args, rank, world):
     gold = {(d["p"], d["k"]): int(d["res64"], 16) for d in g["after"]}
     primes = g["sweep_primes"]
     iters = {"fp64": args.sweep_iters, "ntt": args.sweep_ntt_iters}
-    rows, walls = [], {"fp64": 0.0, "ntt": 0.0}
+    rows, walls, h2d = [], {"fp64": 0.0, "ntt": 0.0}, {"fp64": 0, "ntt": 0}
     llgpu.run(primes[0], iters=64 * args.warmup, n=SWEEP_N)  # warm-up
     barrier(world)
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
@@ -518,9 +536,12 @@ def bench_sweep(args, rank, world):
                 n = SWEEP_N if engine == "fp64" else max(SWEEP_N, llgpu.ntt_length(p))
                 chk = llgpu.run(p, iters=1000, n=n, engine=engine)
                 match = chk["status"] == 0 and chk["res64"] == gold[(p, 1000)]
+                llgpu.release_cached()  # each timed run cold: tables and buffers inside it
+                h0 = llgpu.h2d_bytes()
                 t0 = time.perf_counter()
                 r = llgpu.run(p, iters=iters[engine], n=n, engine=engine)
                 walls[engine] += time.perf_counter() - t0
+                h2d[engine] += llgpu.h2d_bytes() - h0
                 assert r["status"] == 0, (p, engine, r)
                 row[engine] = {"n_used": r["n"], "escalations": r["escalations"],
                                "max_roundoff": round(r["max_err"], 5),
@@ -548,7 +569,7 @@ def bench_sweep(args, rank, world):
         "e2e": {"value": round(1e6 * walls[lead] / (iters[lead] * len(primes)), 3), "unit": "us/iteration",
                 "call": "llg_run(p, K, engine, n) per prime through the C-ABI: tables, s_0 upload, every "
                         "attempt (escalations included), residue rebuilt on the device, result struct back",
-                "h2d_bytes_per_step": sum(4 * SWEEP_N for _ in primes), "d2h_bytes_per_step": 128 * len(primes)},
+                "h2d_bytes_per_step": h2d[lead], "d2h_bytes_per_step": 128 * len(primes)},
         "clocks": clk.summary(),
     }
 

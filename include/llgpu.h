@@ -204,6 +204,16 @@ int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* digits_out,
  * counterpart. */
 int llg_measure_peak(int which, double* ops_per_s);
 
+/* Frees the two-pass test that llg_run keeps, with its tables, buffers and graphs, after a
+ * single-exponent call (one per engine, for the next call on the same exponent, length and split
+ * on the same device). Idle memory of up to ~30 bytes a digit is otherwise held until then. */
+void llg_release_cached(void);
+
+/* Bytes the library has copied from host to device since it was loaded, all threads together
+ * (tables, job lists, residues handed in). Read before and after a call to count that call's
+ * uploads. Diagnostic; no reference counterpart. */
+uint64_t llg_h2d_bytes(void);
+
 #ifdef __cplusplus
 }
 #endif

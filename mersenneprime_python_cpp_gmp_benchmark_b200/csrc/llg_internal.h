@@ -73,6 +73,9 @@ struct NttConst {
 cudaError_t launch_small_ntt(int log_n, const SmallJob* jobs, int njobs, const uint64_t* qtw, NttConst K,
                              int64_t* digits, SmallResult* results, cudaStream_t st);
 
+// Adds `bytes` to the library's host-to-device copy count (llg_h2d_bytes).
+void count_h2d(size_t bytes);
+
 // Digits (int32, natural order, within one of balanced) at length n of the residue s in d_words
 // (ceil(p/64) little-endian limbs, s < 2^p), formed on the GPU; enqueued on st. n <= p, digits of
 // at most 30 bits.

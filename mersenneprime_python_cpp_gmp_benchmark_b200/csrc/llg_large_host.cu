@@ -91,6 +91,7 @@ template <class T>
 cudaError_t upload(T** d, const std::vector<T>& h) {
     cudaError_t e = cudaMalloc(d, h.size() * sizeof(T));
     if (e != cudaSuccess) return e;
+    count_h2d(h.size() * sizeof(T));
     return cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
 }
 
@@ -255,8 +256,14 @@ cudaError_t LargeTest::init(uint64_t p_, uint64_t n, int log_c, int rows_) {
 
 cudaError_t LargeTest::start(const std::vector<int>& d, cudaStream_t st) {
     cudaError_t e;
+    count_h2d(d.size() * sizeof(int));
     if ((e = cudaMemcpyAsync(digits, d.data(), d.size() * sizeof(int), cudaMemcpyHostToDevice, st))) return e;
     return start_device(st);
+}
+
+cudaError_t LargeTest::start_seed(cudaStream_t st) {
+    cudaError_t e = seed_digits_device(digits, N, st);
+    return e ? e : start_device(st);
 }
 
 cudaError_t LargeTest::start_device(cudaStream_t st) {
@@ -332,6 +339,7 @@ cudaError_t LargeTest::diag_withhold_wrap(unsigned long long spin_limit, cudaStr
     // tickets start at 1: ticket 0, the wrap-around job, is never handed out, so tile 0 and the
     // last tile wait for its flag until their limit runs out; every index stays that of a tile
     const unsigned one = 1u;
+    count_h2d(sizeof one);
     if ((e = cudaMemcpyAsync(&ctl->ticket[h.epoch & 1u], &one, sizeof one, cudaMemcpyHostToDevice, st))) return e;
     LargeArgs a = args;
     a.spin_limit = spin_limit;
@@ -400,6 +408,14 @@ std::vector<int> seed_digits(uint64_t n) {
     std::vector<int> d(n, 0);
     d[0] = 4;
     return d;
+}
+
+// The same digits written on the device: zero, then the low byte of digit 0 set to 4 (int32,
+// little-endian). No host buffer and no host-to-device copy of N zero digits.
+cudaError_t seed_digits_device(int* digits, uint64_t n, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(digits, 0, (size_t)n * sizeof(int), st);
+    if (!e) e = cudaMemsetAsync(digits, 4, 1, st);
+    return e;
 }
 
 }  // namespace llg
@@ -495,6 +511,7 @@ cudaError_t NttLargeTest::init(uint64_t p_, int log_n) {
         if (er) return er;
         mem[nmem++] = d;
         *dptr = static_cast<decltype(vec.data())>(d);
+        count_h2d(bytes);
         return cudaMemcpy(d, vec.data(), bytes, cudaMemcpyHostToDevice);
     };
     auto alloc = [&](size_t bytes, void** d) -> cudaError_t {
@@ -583,8 +600,14 @@ cudaError_t NttLargeTest::init(uint64_t p_, int log_n) {
 
 cudaError_t NttLargeTest::start(const std::vector<int>& d, cudaStream_t st) {
     cudaError_t e;
+    count_h2d(d.size() * sizeof(int));
     if ((e = cudaMemcpyAsync(digits, d.data(), d.size() * sizeof(int), cudaMemcpyHostToDevice, st))) return e;
     return start_device(st);
+}
+
+cudaError_t NttLargeTest::start_seed(cudaStream_t st) {
+    cudaError_t e = seed_digits_device(digits, N, st);
+    return e ? e : start_device(st);
 }
 
 cudaError_t NttLargeTest::start_device(cudaStream_t st) {

@@ -204,6 +204,7 @@ extern "C" int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* 
         stage_table<int>(L.sB - o, (size_t)C, [&](size_t i) { return (int)sBb(i); });
         // pageable source: the copy has consumed the stage once the stream has finished it
         e = cudaMemcpyAsync(base + o, g_stage, L.end - o, cudaMemcpyHostToDevice, st);
+        count_h2d(L.end - o);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) {
             cudaStreamSynchronize(st);
@@ -253,6 +254,7 @@ extern "C" int llg_run_noalloc(uint64_t p, uint64_t iters, uint32_t n, int32_t* 
     static const int32_t four = 4;
     if ((e = cudaMemsetAsync(digits_out, 0, N * sizeof(int32_t), st)) != cudaSuccess)
         return fail_enqueued("clearing digits_out", e);
+    count_h2d(sizeof four);
     if ((e = cudaMemcpyAsync(digits_out, &four, sizeof four, cudaMemcpyHostToDevice, st)) != cudaSuccess)
         return fail_enqueued("writing s_0", e);
     if ((e = cudaMemsetAsync(A.ctl, 0, sizeof(LargeCtl), st)) != cudaSuccess) return fail_enqueued("clearing the control block", e);

@@ -366,6 +366,7 @@ extern "C" int llg_residue_from_digits_device(uint64_t p, uint32_t n, const int3
     scan_maps<<<1, kScanThreads, 0, st>>>(maps, nc, cin, top_carry);
     apply_chunks<<<(unsigned)((nc + B - 1) / B), B, 0, st>>>(U, e, cin, nw, nc, F);
     fold_kernel<<<1, 32, 0, st>>>(F, nw, p, top, top_carry, status);
+    count_h2d(sizeof init_flags);
     cudaMemcpyAsync(flags, init_flags, sizeof init_flags, cudaMemcpyHostToDevice, st);
     check_kernel<<<(unsigned)((nw + B - 1) / B), B, 0, st>>>(F, nw, p, flags);
     unsigned hflags[2] = {0, 0};

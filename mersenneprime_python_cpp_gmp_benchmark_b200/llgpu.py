@@ -72,6 +72,10 @@ def lib() -> ctypes.CDLL:
         L.llg_batch_results.argtypes = [ctypes.c_void_p, P(LlgResult), P(u64), sz]
         L.llg_batch_errlog.argtypes = [ctypes.c_void_p, P(ctypes.c_float), sz, P(sz)]
         L.llg_measure_peak.argtypes = [ctypes.c_int, P(dbl)]
+        L.llg_h2d_bytes.argtypes = []
+        L.llg_h2d_bytes.restype = u64
+        L.llg_release_cached.argtypes = []
+        L.llg_release_cached.restype = None
         L.llg_batch_device_ms.argtypes = [ctypes.c_void_p, P(ctypes.c_float)]
         L.llg_batch_destroy.argtypes = [ctypes.c_void_p]
         L.llg_run_noalloc.argtypes = [u64, u64, u32, ctypes.c_void_p, P(dbl), ctypes.c_void_p]
@@ -122,6 +126,16 @@ def measure_peak(which="fp64"):
     v = ctypes.c_double()
     _check(lib().llg_measure_peak(0 if which == "fp64" else 1, ctypes.byref(v)))
     return v.value
+
+
+def h2d_bytes():
+    """Bytes the library has copied from host to device since it was loaded (all threads)."""
+    return int(lib().llg_h2d_bytes())
+
+
+def release_cached():
+    """Frees the two-pass test llg_run keeps for a repeated call on the same exponent."""
+    lib().llg_release_cached()
 
 
 def fft_length(p, max_bpw=0.0):

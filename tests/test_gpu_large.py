@@ -434,3 +434,28 @@ def test_mixed_large_load_and_interim(gpu, oracle):
     assert mid["iters"] == 150 and r["iters"] == 200 and r["n"] == 5 << 18
     assert r["res64"] == gpu.run(p, iters=200, n=5 << 18)["res64"]
     assert mid["res64"] == gpu.run(p, iters=150, n=1 << 21)["res64"]
+
+
+def test_repeated_call_reuses_the_kept_test_exactly(gpu):
+    """llg_run keeps its last two-pass test for the next call on the same exponent, length and
+    split: the repeat uploads no tables and gives the same residues, at other iteration counts too
+    (each checked against the reference GMP engine); llg_release_cached frees it, and the next call
+    builds a fresh one."""
+    gold = {(d["p"], d["k"]): int(d["res64"], 16) for d in load_json("appendix.json")["after"]}
+    p, n = 1257787, 1 << 16
+    gpu.release_cached()
+    h0 = gpu.h2d_bytes()
+    a = gpu.run(p, iters=1000, n=n)
+    h1 = gpu.h2d_bytes()
+    b = gpu.run(p, iters=1000, n=n)
+    h2 = gpu.h2d_bytes()
+    c = gpu.run(p, iters=10000, n=n)
+    d = gpu.run(p, iters=240, n=n)
+    for r, k in ((a, 1000), (b, 1000), (c, 10000), (d, 240)):
+        assert r["status"] == 0 and r["n"] == n and r["res64"] == gold[(p, k)], (k, r)
+    assert h1 - h0 > 10000       # tables of the fresh test (~22 KB at 2^16)
+    assert h2 - h1 < 1000        # the kept test: no tables again
+    gpu.release_cached()
+    h3 = gpu.h2d_bytes()
+    e = gpu.run(p, iters=1000, n=n)
+    assert gpu.h2d_bytes() - h3 > 10000 and e["res64"] == gold[(p, 1000)]
