@@ -207,6 +207,23 @@ __device__ __forceinline__ double i2d_shift(long long x) {
     return __dsub_rn(__longlong_as_double(x + 0x4338000000000000LL), SH);
 }
 
+// Programmatic dependent launch (griddepcontrol, sm_90 and later): let the next kernel of the
+// stream launch once every block of this one has executed it, and wait until the previous kernel
+// has completed with its memory visible. Both are no-ops in a launch without the programmatic
+// stream serialisation attribute.
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait_previous() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// Asynchronous global -> shared copies (cp.async, completed by cp_async_wait_all, then a barrier
+// before other threads read the data).
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+    static_assert(BYTES == 4 || BYTES == 8 || BYTES == 16, "cp.async sizes");
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(s), "l"(gmem), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // 2^e as a double (normal range).
 __device__ __forceinline__ double pow2(int e) { return __longlong_as_double((long long)(1023 + e) << 52); }
 

@@ -98,6 +98,20 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blo
     const int N = A.N, R = A.R;
     const CtaSync sync;
 
+    // The next pass may launch once every block of this one has started (its blocks then take
+    // the SMs this pass's last wave leaves idle). This pass's own constant tables are requested
+    // (asynchronous copies, completed before the barrier that follows the tile loads) before it
+    // waits for the previous pass to complete; nothing it reads from the state, the control block
+    // or the carry slots is touched before that wait.
+    pdl_launch_dependents();
+    for (int k = t; k < QL; k += T) cp_async<16>(qtw + k, A.qtwC + k);
+    for (int k = t; k < C; k += T) {
+        cp_async<8>(swB + k, A.wB + k);
+        if (MODE != LARGE_INIT) cp_async<8>(siwB + k, A.iwB + k);
+        cp_async<4>(ssB + k, A.sB + k);
+    }
+    pdl_wait_previous();
+
     if (t == 0) {
         const unsigned ep = *reinterpret_cast<volatile unsigned*>(&A.ctl->epoch);
         s_epoch = ep;
@@ -148,12 +162,8 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blo
             const int2 d = *reinterpret_cast<const int2*>(A.digits + 2 * m);
             v[i] = make_double2((double)d.x, (double)d.y);
         }
-        for (int k = t; k < QL; k += T) qtw[k] = A.qtwC[k];
-        for (int k = t; k < C; k += T) {
-            swB[k] = __ldg(A.wB + k);
-            ssB[k] = __ldg(A.sB + k);
-        }
-        __syncthreads();
+        cp_async_wait_all();
+        __syncthreads();  // the tables are in shared memory
     } else {
         // ---- the tile's rows, straight into registers: thread (row, tr) holds positions
         //      tr E .. tr E + E-1 (the forward FFT's output order), G rows per 16 G-byte run ----
@@ -162,15 +172,8 @@ __global__ void __launch_bounds__(large_row_threads(LOG_C, G), large_row_min_blo
 #pragma unroll
             for (int j = 0; j < E; ++j) v[j] = __ldcg(lp + (size_t)j * R);
         }
-        // the twiddle and column-weight tables (L2-resident) are fetched while the rows' loads are
-        // in flight
-        for (int k = t; k < QL; k += T) qtw[k] = A.qtwC[k];
-        for (int k = t; k < C; k += T) {
-            swB[k] = __ldg(A.wB + k);
-            siwB[k] = __ldg(A.iwB + k);
-            ssB[k] = __ldg(A.sB + k);
-        }
-        __syncthreads();
+        cp_async_wait_all();
+        __syncthreads();  // the tables are in shared memory
         inverse_from<GC, GC::P - 1, false, CtaSync, G, LE>(v, buf, qtw, tr, sync);
 
         // ---- hop 1: unweight, round, round-off, two-digit chain from zero; hop 2 for rows fed
@@ -331,6 +334,9 @@ __global__ void __launch_bounds__(2 * (1 << LOG_R) / (1 << kLargeLogE), (LOG_R <
     using ColSync = typename std::conditional<(TC >= 32), NamedSync, CtaSync>::type;
     ColSync gsync;
     if constexpr (TC >= 32) gsync = NamedSync{1u + (unsigned)half, (unsigned)TC};
+    // as in the row pass: the next pass may launch once every block has started; the constant
+    // tables are read before waiting for the previous pass
+    pdl_launch_dependents();
     for (int k = t; k < QL; k += 2 * TC) qtw[k] = A.qtwR[k];
     double2* col = A.V + (size_t)__ldg(A.pos_of_c + c) * R;
     // four-step twiddle w_M^{a c} for a = tc + TC i, factored as w_M^{c tc} * w_M^{c TC i}: one
@@ -338,6 +344,7 @@ __global__ void __launch_bounds__(2 * (1 << LOG_R) / (1 << kLargeLogE), (LOG_R <
     double2* ptab = qtw + QL + half * E;
     for (int i = tc; i < E; i += TC) ptab[i] = twiddle_M(A, (uint32_t)c * (uint32_t)(TC * i), false);
     const double2 q = twiddle_M(A, (uint32_t)c * (uint32_t)tc, false);
+    pdl_wait_previous();
     double2 v[E];
 #pragma unroll
     for (int i = 0; i < E; ++i) v[i] = active ? col[tc + TC * i] : make_double2(0.0, 0.0);
@@ -434,6 +441,7 @@ __global__ void __launch_bounds__(2 * R0 * (1 << LOG_L) / (1 << kLargeLogE), (2 
     // barriers: 1 + half for the column's threads, 3 + half R0 + seg for one segment's
     const NamedSync hsync{1u + (unsigned)half, (unsigned)TC};
     const NamedSync ssync{3u + (unsigned)(half * R0 + seg), (unsigned)TL};
+    pdl_launch_dependents();  // as in large_col: constant tables before the wait
     for (int k = t; k < QLL; k += 2 * TC) qtwL[k] = A.qtwL[k];
     for (int k = t; k < QLR; k += 2 * TC) qtwR[k] = A.qtwR[k];
     if (t < R0 * R0) {
@@ -449,6 +457,7 @@ __global__ void __launch_bounds__(2 * R0 * (1 << LOG_L) / (1 << kLargeLogE), (2 
     for (int i = th; i < E; i += TC) ptab[i] = twiddle_M(A, (uint32_t)c * (uint32_t)(TL * i), false);
     const uint32_t a0 = (uint32_t)(seg * L + tl);
     const double2 q = twiddle_M(A, (uint32_t)c * a0, false);
+    pdl_wait_previous();
     double2 v[E];
 #pragma unroll
     for (int i = 0; i < E; ++i) v[i] = active ? col[a0 + TL * i] : make_double2(0.0, 0.0);
@@ -599,10 +608,31 @@ static cudaError_t col_mixed_attr() {
     return e;
 }
 
+// Launch with programmatic stream serialisation at the power-of-two lengths: the kernel may start
+// while the previous kernel of the stream finishes (griddepcontrol in the kernels orders their
+// state accesses after it). At the R0 2^k lengths (logN < 0) it measured slower (5 x 2^18: 37.2 ->
+// 40.7 us per squaring, against 154.1 -> 148.9 at 2^23), so those launch plainly and the
+// griddepcontrol instructions are no-ops.
+template <class... KArgs>
+static cudaError_t launch_pdl(void (*kernel)(KArgs...), int grid, int block, size_t smem, cudaStream_t st,
+                              const LargeArgs& a) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = a.logN > 0 ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, a);
+}
+
 template <int R0, int LOG_L>
 static cudaError_t col_mixed_t(const LargeArgs& a, cudaStream_t st) {
-    large_col_mixed<R0, LOG_L><<<a.C / 2 + 1, col_mixed_threads<R0, LOG_L>(), col_mixed_smem<R0, LOG_L>(), st>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(large_col_mixed<R0, LOG_L>, a.C / 2 + 1, col_mixed_threads<R0, LOG_L>(),
+                      col_mixed_smem<R0, LOG_L>(), st, a);
 }
 
 // INIT: one block per tile. ITER / FINAL: one block more, for the wrap-around job (grid == 0), or
@@ -610,14 +640,12 @@ static cudaError_t col_mixed_t(const LargeArgs& a, cudaStream_t st) {
 template <int LOG_C, int G, int MODE>
 static cudaError_t row_t(const LargeArgs& a, cudaStream_t st, int grid) {
     if (grid <= 0) grid = a.nblocks + (MODE == LARGE_INIT ? 0 : 1);
-    large_row<LOG_C, G, MODE><<<grid, large_row_threads(LOG_C, G), row_smem<LOG_C, G>(), st>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(large_row<LOG_C, G, MODE>, grid, large_row_threads(LOG_C, G), row_smem<LOG_C, G>(), st, a);
 }
 
 template <int LOG_R>
 static cudaError_t col_t(const LargeArgs& a, cudaStream_t st) {
-    large_col<LOG_R><<<a.C / 2 + 1, 2 * (1 << LOG_R) / (1 << kLargeLogE), col_smem<LOG_R>(), st>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(large_col<LOG_R>, a.C / 2 + 1, 2 * (1 << LOG_R) / (1 << kLargeLogE), col_smem<LOG_R>(), st, a);
 }
 
 // Opts the kernels of one geometry into their dynamic shared memory (once per device, before
