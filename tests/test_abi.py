@@ -94,6 +94,24 @@ def test_run_without_gpu_fails_loudly():
         pytest.skip("a GPU is present")
 
 
+def test_failed_calls_copy_nothing_and_release_is_safe():
+    """Without a GPU a call fails before any upload (the library's host-to-device count does not
+    move), and releasing the kept two-pass test is a harmless no-op."""
+    from mersenneprime_python_cpp_gmp_benchmark_b200 import llgpu
+    try:
+        llgpu.device_info()
+    except llgpu.LlgError:
+        h0 = llgpu.h2d_bytes()
+        for p, n in ((136279841, 1 << 23), (1257787, 1 << 16), (4423, 0)):
+            with pytest.raises(llgpu.LlgError):
+                llgpu.run(p, iters=10, n=n)
+        assert llgpu.h2d_bytes() == h0
+        llgpu.release_cached()
+        llgpu.release_cached()
+    else:
+        pytest.skip("a GPU is present")
+
+
 def test_pybind_modules_reference_surface():
     import lucaslehmer as ll
     import lucaslehmer_cuda as lc
