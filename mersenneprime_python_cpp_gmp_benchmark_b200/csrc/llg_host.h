@@ -19,7 +19,6 @@ int large_default_log_c(int log_n);
 bool large_split_supported(int log_n, int log_c, int rows);
 int set_error(int code, const char* msg);  // records this thread's llg_last_error() text
 cudaError_t configure_large(int log_c, int g, int log_r);
-std::vector<int> seed_digits(uint64_t n);
 cudaError_t seed_digits_device(int* digits, uint64_t n, cudaStream_t st);  // s_0 = 4, on the device
 // Quarter-wave table of an L-point FFT in the padded layout the kernels read (entry r at qpad(r)).
 std::vector<double2> padded_quarter_table(uint64_t L);
@@ -52,8 +51,7 @@ struct LargeTest {
     // n: the transform length (2^14 .. 2^23, or R0 2^k as large_mixed_length_supported); log_c < 0:
     // the default split; rows == 0: the default rows per row-pass block (power-of-two lengths)
     cudaError_t init(uint64_t p, uint64_t n, int log_c = -1, int rows = 0);
-    cudaError_t start(const std::vector<int>& digits, cudaStream_t st);  // INIT + first squaring
-    cudaError_t start_seed(cudaStream_t st);    // the same from s_0 = 4 written on the device
+    cudaError_t start_seed(cudaStream_t st);    // s_0 = 4 written on the device, INIT + first squaring
     cudaError_t start_device(cudaStream_t st);  // the same from the digits already in `digits`
     cudaError_t step(uint64_t k, cudaStream_t st);                        // k more squarings
     cudaError_t step_plain(uint64_t k, bool dump_last, cudaStream_t st);
@@ -83,7 +81,6 @@ struct NttLargeTest {
 
     ~NttLargeTest();
     cudaError_t init(uint64_t p, int log_n);
-    cudaError_t start(const std::vector<int>& digits, cudaStream_t st);
     cudaError_t start_seed(cudaStream_t st);
     cudaError_t start_device(cudaStream_t st);
     cudaError_t step(uint64_t k, cudaStream_t st);

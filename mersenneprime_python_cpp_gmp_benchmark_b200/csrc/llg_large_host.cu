@@ -254,13 +254,6 @@ cudaError_t LargeTest::init(uint64_t p_, uint64_t n, int log_c, int rows_) {
     return cudaSuccess;
 }
 
-cudaError_t LargeTest::start(const std::vector<int>& d, cudaStream_t st) {
-    cudaError_t e;
-    count_h2d(d.size() * sizeof(int));
-    if ((e = cudaMemcpyAsync(digits, d.data(), d.size() * sizeof(int), cudaMemcpyHostToDevice, st))) return e;
-    return start_device(st);
-}
-
 cudaError_t LargeTest::start_seed(cudaStream_t st) {
     cudaError_t e = seed_digits_device(digits, N, st);
     return e ? e : start_device(st);
@@ -403,15 +396,9 @@ cudaError_t LargeTest::time_passes(uint64_t k, cudaStream_t st, double& row_us, 
     return e;
 }
 
-// Balanced digits of s_0 = 4 (digit 0 holds 4; every digit has >= 3 bits here).
-std::vector<int> seed_digits(uint64_t n) {
-    std::vector<int> d(n, 0);
-    d[0] = 4;
-    return d;
-}
-
-// The same digits written on the device: zero, then the low byte of digit 0 set to 4 (int32,
-// little-endian). No host buffer and no host-to-device copy of N zero digits.
+// The balanced digits of s_0 = 4 (digit 0 holds 4; every digit has >= 3 bits here), written on
+// the device: zero, then the low byte of digit 0 set to 4 (int32, little-endian). No host buffer
+// and no host-to-device copy of N zero digits.
 cudaError_t seed_digits_device(int* digits, uint64_t n, cudaStream_t st) {
     cudaError_t e = cudaMemsetAsync(digits, 0, (size_t)n * sizeof(int), st);
     if (!e) e = cudaMemsetAsync(digits, 4, 1, st);
@@ -596,13 +583,6 @@ cudaError_t NttLargeTest::init(uint64_t p_, int log_n) {
     A.rem = (int)(p & (N - 1));
     A.logN = logN;
     return cudaSuccess;
-}
-
-cudaError_t NttLargeTest::start(const std::vector<int>& d, cudaStream_t st) {
-    cudaError_t e;
-    count_h2d(d.size() * sizeof(int));
-    if ((e = cudaMemcpyAsync(digits, d.data(), d.size() * sizeof(int), cudaMemcpyHostToDevice, st))) return e;
-    return start_device(st);
 }
 
 cudaError_t NttLargeTest::start_seed(cudaStream_t st) {
