@@ -7,10 +7,12 @@ Workloads (synthetic inputs: the exponents themselves, s_0 = 4; no dataset exist
   big     (default) p = 136,279,841 on the two-pass FP64 IBDWT engine at N = 2^23; one step = 1000
           squarings. metric: us per Lucas-Lehmer iteration (lower is better). value: CUDA events on
           the launch stream, the 64 MiB state resident on the device, L2 flushed between steps.
-          e2e: lucaslehmer.fft_res64_after(p, 2000) -- tables, upload of s_0, squarings, exact
-          residue rebuilt on the device, res64 back -- per squaring. The line also carries the
-          other half of the metric as "range" (the range workload below, one timed step; leave it
-          out with --no-range).
+          e2e: lucaslehmer.fft_res64_after(p, 2000) as a cold call -- tables built and uploaded,
+          buffers allocated, s_0 set on the device, graphs captured, squarings, exact residue
+          rebuilt on the device, res64 back -- per squaring; beside it the same call repeated on
+          the two-pass test the library keeps. Host-to-device bytes are the library's own count.
+          The line also carries the other half of the metric as "range" (the range workload below,
+          one timed step; leave it out with --no-range).
   range   every prime p <= 100,001 (9,592 Lucas-Lehmer tests, 28 Mersenne hits), batched whole-test
           kernels bucketed by transform length. One step = every test run to completion.
           metric: tests/s. e2e: lucaslehmer_cuda.lucas_lehmer_batch() on the host list.
