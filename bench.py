@@ -213,8 +213,15 @@ def bench_range(args, rank, world):
     from mersenneprime_python_cpp_gmp_benchmark_b200 import llgpu
     ps_all = sieve(2, RANGE_HI)
     # the range autotuner picks, per whole-test length of the bits-per-digit rule, the fastest of
-    # that length and the next usable ones on this GPU (power of two against {3,5} x 2^k)
-    tuned = llgpu.autotune_range(RANGE_HI, save=False)
+    # that length and the next usable ones on this GPU (power of two against {3,5} x 2^k);
+    # --range-lengths rule keeps the rule's lengths (a profiler's timings would mislead it)
+    if getattr(args, "range_lengths", "tuned") == "rule":
+        for n in {llgpu.fft_length(p) for p in ps_all if p > 2}:
+            if 0 < n <= 12288:
+                llgpu.set_length_choice(n, 0)
+        tuned = {}
+    else:
+        tuned = llgpu.autotune_range(RANGE_HI, save=False)
     from mersenneprime_python_cpp_gmp_benchmark_b200 import replicas
     mine = replicas.shard(ps_all, rank, world)  # independent tests, balanced by squaring cost
     batch = llgpu.Batch(mine)
@@ -762,6 +769,9 @@ def main():
                     help="range: leave out the timing of the reference's own GPU engine")
     ap.add_argument("--no-range", action="store_true",
                     help="big: leave out the range sub-record (the other half of the metric)")
+    ap.add_argument("--range-lengths", choices=("tuned", "rule"), default="tuned",
+                    help="range: autotune the whole-test lengths (default) or keep the bits-per-digit "
+                         "rule's (for profiler runs)")
     ap.add_argument("--split", default="",
                     help="big, FP64: the two-pass split 'log2 row length,rows per block' instead of the "
                          "autotuner's choice (e.g. 10,8)")
